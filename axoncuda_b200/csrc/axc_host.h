@@ -1,0 +1,48 @@
+// Host-only helpers shared by the readers, writers, generators and the driver.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "../../include/axc.h"
+
+namespace axc {
+
+// Owning storage behind an axc_hgraph returned by axc_read_* / axc_gen_* / axc_quotient_hgraph.
+struct HostGraph {
+    uint32_t n = 0;
+    std::vector<uint64_t> off;   // e+1
+    std::vector<uint32_t> pins;  // sources first per hedge
+    std::vector<uint32_t> nsrc;  // e
+    std::vector<float> w;        // e
+};
+
+void publish(HostGraph *hg, axc_hgraph *out);
+
+// splitmix64: seeds independent xoshiro streams per (seed, index) so generators are
+// deterministic under any thread count.
+inline uint64_t splitmix64(uint64_t &x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+struct Rng {  // xoshiro256**
+    uint64_t s[4];
+    explicit Rng(uint64_t seed, uint64_t stream = 0) {
+        uint64_t x = seed ^ (stream * 0xD1B54A32D192ED03ull + 0x8BB84B93962EACC9ull);
+        for (auto &v : s) v = splitmix64(x);
+    }
+    static inline uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t r = rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+        s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+        s[2] ^= t; s[3] = rotl(s[3], 45);
+        return r;
+    }
+    // uniform in [0, m) (Lemire's multiply-shift; m < 2^32)
+    uint32_t below(uint32_t m) { return (uint32_t)(((next() >> 32) * (uint64_t)m) >> 32); }
+    double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+}  // namespace axc

@@ -1,0 +1,559 @@
+// Coarsening kernels: candidate rating, deterministic matching with orphan pairing, group
+// relabelling, and the INCC greedy merge of the coarsest groups.
+//
+// Rating (kernels/coarsening.cu:76-212 restated, node-parallel, no neighbour CSR): for node u,
+// every pin v != u of every hyperedge e incident to u adds floor(w_fx(e)/|e|) to v's score and,
+// when e is inbound to u and v is one of e's destinations, 1 to v's shared-inbound count. The
+// per-node accumulator is an open-addressing table: in shared memory per warp for light nodes,
+// per block for medium ones, in a global scratch region for heavy ones. Candidates failing
+// size(u)+size(v) <= omega or |in(u)|+|in(v)|-shared <= delta are dropped, the symmetric noise of
+// the pair is added, and the top `cnc` by (score desc, id desc) with score > 0 are written.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace axc {
+namespace {
+
+constexpr u32 RT_WARP_W = 256;     // work (incident pins) handled by one warp
+constexpr u32 RT_BLK1_W = 2048;    // block tier 1: table 4096 slots (48 KiB)
+constexpr u32 RT_BLK2_W = 8192;    // block tier 2: table 16384 slots (192 KiB)
+constexpr u32 RT_WARPS = 4;
+constexpr u32 RT_BLOCK = 256;
+
+__global__ void k_rate_work(u32 n, const u64 *__restrict__ toff, const u32 *__restrict__ touch,
+                            const u64 *__restrict__ off, u64 *__restrict__ work) {
+    const u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (u >= n) return;
+    u64 s = 0;
+    for (u64 j = toff[u] + lane; j < toff[u + 1]; j += 32) {
+        u32 h = touch[j];
+        s += off[h + 1] - off[h];
+    }
+    s = warp_sum(s);
+    if (lane == 0) work[u] = s;
+}
+
+__global__ void k_rate_tier(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
+    u32 u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < n) flag[u] = (work[u] > lo && work[u] <= hi) ? 1u : 0u;
+}
+
+struct RateArgs {
+    u32 n, cnc, omega, delta;
+    const u64 *off;
+    const u32 *pins, *nsrc, *wfx;
+    const u64 *toff;
+    const u32 *touch, *nin, *nsize;
+    u32 *pairs, *scores;
+    u32 *status;
+};
+
+// Accumulate node u's neighbour scores into (keys, sc, cm) of size mask+1, using `nt` threads with
+// index t; `scratch` holds per-thread chunk info for the block variant (nullptr: warp variant).
+template <bool WARP>
+__device__ void rate_accumulate(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 t,
+                                u32 nt, u32 *sh_excl, u32 *sh_a, u32 *sh_c, u32 *sh_s, u32 *sh_inb,
+                                u32 *sh_tot) {
+    const u64 t0 = A.toff[u], t1 = A.toff[u + 1];
+    const u32 deg = (u32)(t1 - t0), nin_u = A.nin[u];
+    for (u32 jb = 0; jb < deg; jb += nt) {
+        const u32 j = jb + t;
+        const bool has = j < deg;
+        u32 h = has ? A.touch[t0 + j] : 0;
+        u64 a = has ? A.off[h] : 0;
+        u32 len = has ? (u32)(A.off[h + 1] - a) : 0;
+        u32 c = has ? A.wfx[h] / len : 0;
+        u32 s_end = has ? (u32)A.nsrc[h] : 0;  // sources occupy [0, s_end)
+        u32 inb = (has && j < nin_u) ? 1u : 0u;
+        u32 excl, total;
+        if (WARP) {
+            u32 x = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if ((int)t >= o) x += y;
+            }
+            total = __shfl_sync(0xFFFFFFFFu, x, 31);
+            excl = x - len;
+        } else {
+            // block-wide exclusive scan of len
+            sh_excl[t] = len;
+            __syncthreads();
+            for (u32 o = 1; o < nt; o <<= 1) {
+                u32 y = t >= o ? sh_excl[t - o] : 0;
+                __syncthreads();
+                sh_excl[t] += y;
+                __syncthreads();
+            }
+            excl = sh_excl[t] - len;
+            if (t == nt - 1) *sh_tot = sh_excl[t];
+            __syncthreads();
+            total = *sh_tot;
+            sh_excl[t] = excl;
+            sh_c[t] = c;
+            sh_s[t] = s_end;
+            sh_inb[t] = inb;
+            __syncthreads();
+        }
+        const u32 chunk = (deg - jb) < nt ? (deg - jb) : nt;
+        for (u32 fb = 0; fb < total; fb += nt) {
+            const u32 f = fb + t;
+            const bool ok = f < total;
+            // owner: largest o < chunk with excl_o <= f
+            u32 lo = 0, hi = chunk - 1;
+            if (WARP) {
+                for (int it = 0; it < 5; ++it) {
+                    const u32 mid = (lo + hi + 1) >> 1;
+                    const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
+                    if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
+                }
+            } else {
+                while (lo < hi) {
+                    u32 mid = (lo + hi + 1) >> 1;
+                    if (sh_excl[mid] <= f) lo = mid; else hi = mid - 1;
+                }
+            }
+            const u32 o = lo;
+            u32 hh, cc, ss, ib, eo;
+            if (WARP) {
+                hh = __shfl_sync(0xFFFFFFFFu, h, o);
+                cc = __shfl_sync(0xFFFFFFFFu, c, o);
+                ss = __shfl_sync(0xFFFFFFFFu, s_end, o);
+                ib = __shfl_sync(0xFFFFFFFFu, inb, o);
+                eo = __shfl_sync(0xFFFFFFFFu, excl, o);
+            } else {
+                hh = A.touch[t0 + jb + o];
+                cc = sh_c[o];
+                ss = sh_s[o];
+                ib = sh_inb[o];
+                eo = sh_excl[o];
+            }
+            if (!ok) continue;
+            const u32 i = f - eo;  // position inside hyperedge hh
+            const u32 v = A.pins[A.off[hh] + i];
+            if (v == u) continue;
+            const u32 slot = hash_find_or_insert(keys, mask, v);
+            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            atomicAdd(&sc[slot], cc);
+            if (ib && i >= ss) atomicAdd(&cm[slot], 1u);
+        }
+        if (!WARP) __syncthreads();
+    }
+}
+
+__device__ __forceinline__ u64 cand_key(const RateArgs &A, u32 u, u32 v, u32 s, u32 shared_inb) {
+    if ((u64)A.nsize[u] + A.nsize[v] > A.omega) return 0;
+    if ((u64)A.nin[u] + A.nin[v] - shared_inb > A.delta) return 0;
+    const u32 score = s + pair_noise(u, v);
+    if (score == 0) return 0;
+    return ((u64)score << 32) | v;
+}
+
+__global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u32 *__restrict__ list, u32 nlist) {
+    __shared__ u32 tk[RT_WARPS][2 * RT_WARP_W], ts[RT_WARPS][2 * RT_WARP_W], tc[RT_WARPS][2 * RT_WARP_W];
+    const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 idx = blockIdx.x * RT_WARPS + w;
+    if (idx >= nlist) return;
+    const u32 u = list[idx];
+    u32 *keys = tk[w], *sc = ts[w], *cm = tc[w];
+    u32 W = 0;  // work bound for the table size
+    for (u64 j = A.toff[u] + lane; j < A.toff[u + 1]; j += 32) {
+        u32 h = A.touch[j];
+        W += (u32)(A.off[h + 1] - A.off[h]);
+    }
+    W = warp_sum(W);
+    u32 cap = 64;
+    while (cap < 2 * W) cap <<= 1;
+    for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
+    __syncwarp();
+    rate_accumulate<true>(A, u, keys, sc, cm, cap - 1, lane, 32, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, nullptr);
+    __syncwarp();
+    u64 prev = ~0ull;
+    for (u32 r = 0; r < A.cnc; ++r) {
+        u64 best = 0;
+        for (u32 i = lane; i < cap; i += 32) {
+            u32 v = keys[i];
+            if (v == NONE) continue;
+            u64 k = cand_key(A, u, v, sc[i], cm[i]);
+            if (k < prev && k > best) best = k;
+        }
+        best = warp_max_u64(best);
+        if (lane == 0) {
+            A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
+            A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
+        }
+        prev = best ? best : 0;
+        if (!best) {
+            for (u32 r2 = r + 1 + lane; r2 < A.cnc; r2 += 32) {
+                A.pairs[(u64)u * A.cnc + r2] = NONE;
+                A.scores[(u64)u * A.cnc + r2] = 0;
+            }
+            break;
+        }
+    }
+}
+
+__device__ __forceinline__ u64 block_max_u64(u64 v, u64 *red) {
+    v = warp_max_u64(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        u64 x = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+        x = warp_max_u64(x);
+        if (threadIdx.x == 0) red[32] = x;
+    }
+    __syncthreads();
+    u64 r = red[32];
+    __syncthreads();
+    return r;
+}
+
+// One node per block iteration; table in dynamic smem (gtab == nullptr) or in this block's
+// slice of a global scratch region.
+__global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
+                                                        u32 cap_max, u32 *gtab) {
+    extern __shared__ u32 dyn[];
+    __shared__ u32 sh_excl[RT_BLOCK], sh_c[RT_BLOCK], sh_s[RT_BLOCK], sh_inb[RT_BLOCK], sh_tot;
+    __shared__ u64 red[33];
+    u32 *keys, *sc, *cm;
+    if (gtab) {
+        keys = gtab + (u64)blockIdx.x * 3 * cap_max;
+    } else {
+        keys = dyn;
+    }
+    for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
+        const u32 u = list[idx];
+        // table size from the node's work bound, capped by the node count
+        __shared__ u64 Wsh;
+        if (threadIdx.x == 0) Wsh = 0;
+        __syncthreads();
+        u64 W = 0;
+        for (u64 j = A.toff[u] + threadIdx.x; j < A.toff[u + 1]; j += blockDim.x) {
+            u32 h = A.touch[j];
+            W += A.off[h + 1] - A.off[h];
+        }
+        W = warp_sum(W);
+        if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long *)&Wsh, (unsigned long long)W);
+        __syncthreads();
+        W = Wsh < A.n ? Wsh : A.n;
+        u32 cap = 64;
+        while (cap < 2 * W && cap < cap_max) cap <<= 1;
+        sc = keys + cap;
+        cm = sc + cap;
+        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
+        __syncthreads();
+        rate_accumulate<false>(A, u, keys, sc, cm, cap - 1, threadIdx.x, blockDim.x, sh_excl, nullptr, sh_c,
+                               sh_s, sh_inb, &sh_tot);
+        __syncthreads();
+        u64 prev = ~0ull;
+        for (u32 r = 0; r < A.cnc; ++r) {
+            u64 best = 0;
+            for (u32 i = threadIdx.x; i < cap; i += blockDim.x) {
+                u32 v = keys[i];
+                if (v == NONE) continue;
+                u64 k = cand_key(A, u, v, sc[i], cm[i]);
+                if (k < prev && k > best) best = k;
+            }
+            best = block_max_u64(best, red);
+            if (threadIdx.x == 0) {
+                A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
+                A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
+            }
+            prev = best;
+            if (!best) {
+                for (u32 r2 = r + 1 + threadIdx.x; r2 < A.cnc; r2 += blockDim.x) {
+                    A.pairs[(u64)u * A.cnc + r2] = NONE;
+                    A.scores[(u64)u * A.cnc + r2] = 0;
+                }
+                break;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- matching
+// Rounds of mutual proposals (see or_matching in the oracle for the rule). One cooperative launch
+// runs every round with grid-wide barriers; without cooperative launch each phase is a kernel.
+__device__ __forceinline__ void match_propose(u32 n, u32 cnc, const u32 *pairs, const u32 *mate, u32 *ptr,
+                                              u32 *prop, u64 i0, u64 stride) {
+    for (u64 v = i0; v < n; v += stride) {
+        if (mate[v] != NONE) { prop[v] = NONE; continue; }
+        u32 p = ptr[v];
+        while (p < cnc) {
+            u32 w = pairs[v * cnc + p];
+            if (w == NONE) { p = cnc; break; }
+            if (mate[w] == NONE) break;
+            ++p;
+        }
+        ptr[v] = p;
+        prop[v] = p < cnc ? pairs[v * cnc + p] : NONE;
+    }
+}
+__device__ __forceinline__ void match_accept(u32 n, const u32 *prop, u32 *mate, u32 *changed, u64 i0,
+                                             u64 stride) {
+    for (u64 v = i0; v < n; v += stride) {
+        u32 w = prop[v];
+        if (w != NONE && w > v && prop[w] == v) {
+            mate[v] = w;
+            mate[w] = (u32)v;
+            *changed = 1;
+        }
+    }
+}
+
+__global__ void k_match_coop(u32 n, u32 cnc, const u32 *__restrict__ pairs, u32 *mate, u32 *ptr, u32 *prop,
+                             u32 rounds, u32 *changed) {
+    cg::grid_group grid = cg::this_grid();
+    const u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, stride = (u64)gridDim.x * blockDim.x;
+    for (u32 r = 0; r < rounds; ++r) {
+        match_propose(n, cnc, pairs, mate, ptr, prop, i0, stride);
+        grid.sync();
+        match_accept(n, prop, mate, &changed[r], i0, stride);
+        grid.sync();
+        if (((volatile u32 *)changed)[r] == 0) break;
+    }
+}
+__global__ void k_match_propose(u32 n, u32 cnc, const u32 *pairs, const u32 *mate, u32 *ptr, u32 *prop,
+                                const u32 *changed, u32 r) {
+    if (r > 0 && changed[r - 1] == 0) return;
+    match_propose(n, cnc, pairs, mate, ptr, prop, (u64)blockIdx.x * blockDim.x + threadIdx.x,
+                  (u64)gridDim.x * blockDim.x);
+}
+__global__ void k_match_accept(u32 n, const u32 *prop, u32 *mate, u32 *changed, u32 r) {
+    if (r > 0 && changed[r - 1] == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) changed[r] = 0;
+        return;
+    }
+    match_accept(n, prop, mate, &changed[r], (u64)blockIdx.x * blockDim.x + threadIdx.x,
+                 (u64)gridDim.x * blockDim.x);
+}
+
+__global__ void k_orphan_flags(u32 n, u32 cnc, const u32 *__restrict__ pairs, u32 *__restrict__ flag) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) flag[v] = pairs[(u64)v * cnc] == NONE ? 1u : 0u;
+}
+__global__ void k_gather_size(const u32 *__restrict__ ids, u32 m, const u32 *__restrict__ nsize, u32 *__restrict__ out) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = nsize[ids[i]];
+}
+__global__ void k_orphan_pair(const u32 *__restrict__ ord, u32 m, const u32 *__restrict__ nsize,
+                              const u32 *__restrict__ nin, u32 omega, u32 delta, u32 *__restrict__ mate) {
+    u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m / 2) return;
+    u32 L = ord[k], R = ord[m - 1 - k];
+    if ((u64)nsize[L] + nsize[R] > omega) return;
+    if ((u64)nin[L] + nin[R] > delta) return;
+    mate[L] = R;
+    mate[R] = L;
+}
+__global__ void k_group_heads(u32 n, const u32 *__restrict__ mate, u32 *__restrict__ head) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) head[v] = (mate[v] == NONE || v < mate[v]) ? 1u : 0u;
+}
+__global__ void k_group_assign(u32 n, const u32 *__restrict__ mate, const u32 *__restrict__ gid,
+                               u32 *__restrict__ groups) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    u32 m = mate[v];
+    groups[v] = gid[(m == NONE || v < m) ? v : m];
+}
+
+// ---------------------------------------------------------------- greedy merge (-ipm)
+__global__ void k_group_sums(u32 n, const u32 *__restrict__ groups, const u32 *__restrict__ nsize,
+                             const u32 *__restrict__ nin, u32 *__restrict__ gs, unsigned long long *__restrict__ gi) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    atomicAdd(&gs[groups[v]], nsize[v]);
+    atomicAdd(&gi[groups[v]], (unsigned long long)nin[v]);
+}
+__global__ void k_split64(const u64 *__restrict__ x, const u32 *__restrict__ ids, u32 m, u32 *__restrict__ hi,
+                          u32 *__restrict__ lo) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    u64 v = x[ids ? ids[i] : i];
+    hi[i] = (u32)(v >> 32);
+    lo[i] = (u32)v;
+}
+__global__ void k_gather_sz64(const u32 *__restrict__ ord, u32 m, const u32 *__restrict__ gs, const u64 *__restrict__ gi,
+                              u64 *__restrict__ ss, u64 *__restrict__ si) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    ss[i] = gs[ord[i]];
+    si[i] = gi[ord[i]];
+}
+__global__ void k_pack_rep(const u32 *__restrict__ ord, const u32 *__restrict__ packid, u32 m, u32 *__restrict__ rep) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) atomicMin(&rep[packid[i]], ord[i]);
+}
+__global__ void k_pack_map(const u32 *__restrict__ ord, const u32 *__restrict__ packid, const u32 *__restrict__ rep,
+                           u32 m, u32 *__restrict__ gmap) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) gmap[ord[i]] = rep[packid[i]];
+}
+__global__ void k_self_head(const u32 *__restrict__ gmap, u32 m, u32 *__restrict__ head) {
+    u32 x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < m) head[x] = gmap[x] == x ? 1u : 0u;
+}
+__global__ void k_remap_groups(u32 n, u32 *__restrict__ groups, const u32 *__restrict__ gmap, const u32 *__restrict__ nid) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) groups[v] = nid[gmap[groups[v]]];
+}
+
+}  // namespace
+
+void setup_coarsen_kernels(Ctx &c) {
+    AXC_CUDA(cudaFuncSetAttribute(k_rate_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 16384 * 4));
+}
+
+void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 cnc, u32 *pairs, u32 *scores,
+            u64 *pin_visits) {
+    const u32 n = L.n;
+    if (n == 0) return;
+    size_t m = c.arena.mark();
+    RateArgs A{n, cnc, omega, delta, L.off, L.pins, L.nsrc, wfx, L.toff, L.touch, L.nin, L.nsize, pairs, scores,
+               c.d_status};
+    u64 *work = c.arena.alloc<u64>(n);
+    u32 *flag = c.arena.alloc<u32>(n), *list = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_rate_work, cdiv((u64)n * 32, 256), 256, 0, n, L.toff, L.touch, L.off, work);
+    if (pin_visits) *pin_visits = reduce_sum_u64(c, work, n);
+    // tier: one warp per node, table in static smem
+    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, 0ull, (u64)RT_WARP_W, flag);
+    u32 nl = compact_indices(c, flag, list, n);
+    LAUNCH(c, k_rate_warp, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
+    // tier: one block per node, 4096-slot table in dynamic smem
+    u32 *list2 = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_WARP_W, (u64)RT_BLK1_W, flag);
+    nl = compact_indices(c, flag, list2, n);
+    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 4096 * 4, A, list2, nl, 4096u, (u32 *)nullptr);
+    // tier: one block per node, 16384-slot table in dynamic smem
+    u32 *list3 = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_BLK1_W, (u64)RT_BLK2_W, flag);
+    nl = compact_indices(c, flag, list3, n);
+    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 16384 * 4, A, list3, nl, 16384u, (u32 *)nullptr);
+    // tier: heavy nodes, tables in a global scratch slice per resident block
+    u32 *list4 = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_BLK2_W, ~0ull, flag);
+    nl = compact_indices(c, flag, list4, n);
+    if (nl) {
+        u64 wmax = reduce_max_u64(c, work, n);
+        if (wmax > n) wmax = n;  // distinct neighbours never exceed the node count
+        u32 cap = 64;
+        while (cap < 2 * wmax && cap < (1u << 30)) cap <<= 1;
+        u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
+        u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
+        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+    }
+    check_status(c);
+    c.arena.release(m);
+}
+
+u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u32 *nin, u32 omega, u32 delta,
+             u32 rounds, u32 *groups) {
+    if (n == 0) return 0;
+    size_t m = c.arena.mark();
+    u32 *mate = c.arena.alloc<u32>(n), *ptr = c.arena.alloc<u32>(n), *prop = c.arena.alloc<u32>(n);
+    u32 *changed = c.arena.alloc<u32>(rounds + 1);
+    fill_u32(c, mate, NONE, n);
+    AXC_CUDA(cudaMemsetAsync(ptr, 0, (size_t)n * 4, c.stream));
+    AXC_CUDA(cudaMemsetAsync(changed, 0, (size_t)(rounds + 1) * 4, c.stream));
+    bool done = false;
+    if (c.coop_supported) {
+        int per_sm = 0;
+        AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_coop, 256, 0));
+        u32 grid = (u32)per_sm * c.sms;
+        u32 need = cdiv(n, 256);
+        if (grid > need) grid = need;
+        if (grid >= 1 && per_sm > 0) {
+            void *args[] = {(void *)&n, (void *)&cnc, (void *)&pairs, (void *)&mate, (void *)&ptr,
+                            (void *)&prop, (void *)&rounds, (void *)&changed};
+            AXC_CUDA(cudaLaunchCooperativeKernel((void *)k_match_coop, grid, 256, args, 0, c.stream));
+            c.launches++;
+            done = true;
+        }
+    }
+    if (!done) {
+        u32 grid = cdiv(n, 256);
+        for (u32 r = 0; r < rounds; ++r) {
+            LAUNCH(c, k_match_propose, grid, 256, 0, n, cnc, pairs, mate, ptr, prop, changed, r);
+            LAUNCH(c, k_match_accept, grid, 256, 0, n, prop, mate, changed, r);
+        }
+    }
+    // orphans
+    u32 *flag = c.arena.alloc<u32>(n), *orph = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_orphan_flags, cdiv(n, 256), 256, 0, n, cnc, pairs, flag);
+    u32 mo = compact_indices(c, flag, orph, n);
+    if (mo >= 2) {
+        u32 *key = c.arena.alloc<u32>(mo);
+        LAUNCH(c, k_gather_size, cdiv(mo, 256), 256, 0, orph, mo, nsize, key);
+        u32 maxs = reduce_max_u32(c, key, mo);
+        radix_sort_pairs(c, key, orph, mo, bits_for(maxs));
+        LAUNCH(c, k_orphan_pair, cdiv(mo / 2, 256), 256, 0, orph, mo, nsize, nin, omega, delta, mate);
+    }
+    // relabel in order of the smallest member
+    u32 *head = flag, *gid = orph;
+    LAUNCH(c, k_group_heads, cdiv(n, 256), 256, 0, n, mate, head);
+    scan_excl_u32(c, head, gid, n);
+    u64 tail[2];
+    {
+        u32 *d = c.arena.alloc<u32>(2);
+        AXC_CUDA(cudaMemcpyAsync(d, gid + n - 1, 4, cudaMemcpyDeviceToDevice, c.stream));
+        AXC_CUDA(cudaMemcpyAsync(d + 1, head + n - 1, 4, cudaMemcpyDeviceToDevice, c.stream));
+        fetch(c, tail, d, 8);
+    }
+    const u32 *t32 = (const u32 *)tail;
+    u32 ng = t32[0] + t32[1];
+    LAUNCH(c, k_group_assign, cdiv(n, 256), 256, 0, n, mate, gid, groups);
+    c.arena.release(m);
+    return ng;
+}
+
+u32 greedy_merge_groups(Ctx &c, u32 n, const u32 *nsize, const u32 *nin, u32 *groups, u32 ng, u32 omega,
+                        u32 delta) {
+    if (n == 0 || ng < 2) return ng;
+    size_t mk = c.arena.mark();
+    const u32 m = ng;
+    u32 *gs = c.arena.alloc<u32>(m);
+    u64 *gi = c.arena.alloc<u64>(m);
+    AXC_CUDA(cudaMemsetAsync(gs, 0, (size_t)m * 4, c.stream));
+    AXC_CUDA(cudaMemsetAsync(gi, 0, (size_t)m * 8, c.stream));
+    LAUNCH(c, k_group_sums, cdiv(n, 256), 256, 0, n, groups, nsize, nin, gs, (unsigned long long *)gi);
+    // order by (size, inbound, id): ids ascending, stable by inbound (64-bit), stable by size
+    u32 *ord = c.arena.alloc<u32>(m), *hi = c.arena.alloc<u32>(m), *lo = c.arena.alloc<u32>(m);
+    iota_u32(c, ord, m);
+    LAUNCH(c, k_split64, cdiv(m, 256), 256, 0, gi, (const u32 *)nullptr, m, hi, lo);
+    radix_sort_pairs64(c, hi, lo, ord, m, 32, 32);
+    LAUNCH(c, k_gather_size, cdiv(m, 256), 256, 0, ord, m, gs, lo);
+    radix_sort_pairs(c, lo, ord, m, 32);
+    u64 *ss = c.arena.alloc<u64>(m), *si = c.arena.alloc<u64>(m);
+    LAUNCH(c, k_gather_sz64, cdiv(m, 256), 256, 0, ord, m, gs, gi, ss, si);
+    u32 *msc = c.arena.alloc<u32>(m), *packid = c.arena.alloc<u32>(m), *rep = c.arena.alloc<u32>(m);
+    greedy_pack(c, ss, si, m, (u64)omega, (u64)delta, packid);
+    fill_u32(c, rep, NONE, m);
+    LAUNCH(c, k_pack_rep, cdiv(m, 256), 256, 0, ord, packid, m, rep);
+    u32 *gmap = hi;
+    LAUNCH(c, k_pack_map, cdiv(m, 256), 256, 0, ord, packid, rep, m, gmap);
+    u32 *head = lo, *nid = msc;
+    LAUNCH(c, k_self_head, cdiv(m, 256), 256, 0, gmap, m, head);
+    scan_excl_u32(c, head, nid, m);
+    u32 t[2];
+    {
+        u32 *d = c.arena.alloc<u32>(2);
+        AXC_CUDA(cudaMemcpyAsync(d, nid + m - 1, 4, cudaMemcpyDeviceToDevice, c.stream));
+        AXC_CUDA(cudaMemcpyAsync(d + 1, head + m - 1, 4, cudaMemcpyDeviceToDevice, c.stream));
+        u64 tmp;
+        fetch(c, &tmp, d, 8);
+        memcpy(t, &tmp, 8);
+    }
+    const u32 newg = t[0] + t[1];
+    LAUNCH(c, k_remap_groups, cdiv(n, 256), 256, 0, n, groups, gmap, nid);
+    c.arena.release(mk);
+    return newg;
+}
+
+}  // namespace axc

@@ -1,0 +1,381 @@
+// Host side of the C ABI: hypergraph readers and writers, partition files, the quotient
+// hypergraph used by `-s`, and the seeded synthetic generators.
+//
+// Readers follow the reference's HyperGraph loaders (includes/hgraph.hpp:707-743 .snn,
+// 805-854 .axh, 936-1013 .hgr) including their quirks: .hgr nets have no sources, singleton
+// nets are skipped, vertex weights are ignored, ids are 1-based in the file. Unlike the
+// reference (which reads 4 bytes per call through std::ifstream) the binary formats are read
+// with one bulk read and parsed in memory.
+#include "axc_host.h"
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace axc {
+
+static bool read_file(const char *path, std::vector<char> &buf) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return false;
+    if (std::fseek(f, 0, SEEK_END) != 0) { std::fclose(f); return false; }
+    long sz = std::ftell(f);
+    if (sz < 0) { std::fclose(f); return false; }
+    std::rewind(f);
+    buf.resize((size_t)sz);
+    size_t got = sz ? std::fread(buf.data(), 1, (size_t)sz, f) : 0;
+    std::fclose(f);
+    return got == (size_t)sz;
+}
+
+void publish(HostGraph *hg, axc_hgraph *out) {
+    out->n = hg->n;
+    out->e = (uint32_t)hg->nsrc.size();
+    out->hedge_off = hg->off.data();
+    out->pins = hg->pins.data();
+    out->src_count = hg->nsrc.data();
+    out->hedge_w = hg->w.data();
+    out->_owner = hg;
+}
+
+}  // namespace axc
+
+using namespace axc;
+
+extern "C" void axc_free_hgraph(axc_hgraph *g) {
+    if (!g) return;
+    delete static_cast<HostGraph *>(g->_owner);
+    std::memset(g, 0, sizeof(*g));
+}
+
+// .snn: u32 n, u32 E, then per hedge {u32 dst_count, u32 src, u32 dst[dst_count], f32 w}
+extern "C" int axc_read_snn(const char *path, axc_hgraph *out) {
+    if (!path || !out) return AXC_EINVAL;
+    std::vector<char> buf;
+    if (!read_file(path, buf)) return AXC_EIO;
+    if (buf.size() < 8) return AXC_EFORMAT;
+    const uint8_t *p = (const uint8_t *)buf.data(), *end = p + buf.size();
+    auto r32 = [&](uint32_t &v) -> bool {
+        if (end - p < 4) return false;
+        std::memcpy(&v, p, 4); p += 4; return true;
+    };
+    uint32_t n, E;
+    if (!r32(n) || !r32(E)) return AXC_EFORMAT;
+    auto *hg = new HostGraph();
+    hg->n = n;
+    hg->off.reserve((size_t)E + 1);
+    hg->nsrc.reserve(E);
+    hg->w.reserve(E);
+    hg->off.push_back(0);
+    hg->pins.reserve((buf.size() - 8) / 4);
+    for (uint32_t i = 0; i < E; ++i) {
+        uint32_t dstc, src;
+        if (!r32(dstc) || !r32(src)) { delete hg; return AXC_EFORMAT; }
+        if (dstc < 1 || src >= n) { delete hg; return AXC_EFORMAT; }  // hgraph.hpp:145 needs >= 1 destination
+        if ((size_t)(end - p) < (size_t)dstc * 4 + 4) { delete hg; return AXC_EFORMAT; }
+        hg->pins.push_back(src);
+        size_t base = hg->pins.size();
+        hg->pins.resize(base + dstc);
+        std::memcpy(hg->pins.data() + base, p, (size_t)dstc * 4);
+        p += (size_t)dstc * 4;
+        for (size_t k = base; k < base + dstc; ++k)
+            if (hg->pins[k] >= n) { delete hg; return AXC_EFORMAT; }
+        float w; std::memcpy(&w, p, 4); p += 4;
+        hg->nsrc.push_back(1);
+        hg->w.push_back(w);
+        hg->off.push_back(hg->pins.size());
+    }
+    publish(hg, out);
+    return AXC_OK;
+}
+
+// .axh: u32 n, u32 E, then per hedge {u32 pin_count, u32 src_count, u32 pins[], f32 w}
+extern "C" int axc_read_axh(const char *path, axc_hgraph *out) {
+    if (!path || !out) return AXC_EINVAL;
+    std::vector<char> buf;
+    if (!read_file(path, buf)) return AXC_EIO;
+    if (buf.size() < 8) return AXC_EFORMAT;
+    const uint8_t *p = (const uint8_t *)buf.data(), *end = p + buf.size();
+    auto r32 = [&](uint32_t &v) -> bool {
+        if (end - p < 4) return false;
+        std::memcpy(&v, p, 4); p += 4; return true;
+    };
+    uint32_t n, E;
+    if (!r32(n) || !r32(E)) return AXC_EFORMAT;
+    auto *hg = new HostGraph();
+    hg->n = n;
+    hg->off.push_back(0);
+    for (uint32_t i = 0; i < E; ++i) {
+        uint32_t pc, sc;
+        if (!r32(pc) || !r32(sc)) { delete hg; return AXC_EFORMAT; }
+        // hgraph.hpp:826-827 (src_count >= 1, pin_count >= src_count) and :145 (>= 1 destination)
+        if (sc == 0 || pc < sc || pc == sc) { delete hg; return AXC_EFORMAT; }
+        if ((size_t)(end - p) < (size_t)pc * 4 + 4) { delete hg; return AXC_EFORMAT; }
+        size_t base = hg->pins.size();
+        hg->pins.resize(base + pc);
+        std::memcpy(hg->pins.data() + base, p, (size_t)pc * 4);
+        p += (size_t)pc * 4;
+        for (size_t k = base; k < base + pc; ++k)
+            if (hg->pins[k] >= n) { delete hg; return AXC_EFORMAT; }
+        float w; std::memcpy(&w, p, 4); p += 4;
+        hg->nsrc.push_back(sc);
+        hg->w.push_back(w);
+        hg->off.push_back(hg->pins.size());
+    }
+    publish(hg, out);
+    return AXC_OK;
+}
+
+// .hgr (hMETIS): "E V [fmt]" header, E net lines "[w] v1 v2 ...", '%' comments.
+extern "C" int axc_read_hgr(const char *path, axc_hgraph *out) {
+    if (!path || !out) return AXC_EINVAL;
+    std::vector<char> buf;
+    if (!read_file(path, buf)) return AXC_EIO;
+    buf.push_back('\n');
+    const char *p = buf.data(), *end = buf.data() + buf.size();
+    // next data line: skip blank and '%' lines (hgraph.hpp:940-950)
+    auto next_line = [&](const char *&ls, const char *&le) -> bool {
+        while (p < end) {
+            const char *s = p;
+            const char *e = (const char *)std::memchr(p, '\n', (size_t)(end - p));
+            if (!e) e = end;
+            p = e + 1;
+            const char *q = s;
+            while (q < e && (*q == ' ' || *q == '\t')) ++q;
+            const char *ee = e;
+            if (ee > q && ee[-1] == '\r') --ee;
+            if (q == ee || *q == '%') continue;
+            ls = q; le = ee;
+            return true;
+        }
+        return false;
+    };
+    auto parse_u64 = [](const char *&q, const char *le, uint64_t &v) -> bool {
+        while (q < le && (*q == ' ' || *q == '\t')) ++q;
+        if (q >= le || *q < '0' || *q > '9') return false;
+        uint64_t x = 0;
+        while (q < le && *q >= '0' && *q <= '9') {
+            x = x * 10 + (uint64_t)(*q - '0');
+            if (x > 0xFFFFFFFFFFull) return false;
+            ++q;
+        }
+        v = x;
+        return true;
+    };
+    const char *ls, *le;
+    if (!next_line(ls, le)) return AXC_EFORMAT;  // "Empty .hgr file"
+    uint64_t E64, V64, fmt = 0;
+    const char *q = ls;
+    if (!parse_u64(q, le, E64) || !parse_u64(q, le, V64)) return AXC_EFORMAT;
+    if (E64 > 0xFFFFFFFFull || V64 > 0xFFFFFFFFull) return AXC_EFORMAT;
+    if (!parse_u64(q, le, fmt)) fmt = 0;
+    const bool edge_w = (fmt == 1 || fmt == 11);
+    auto *hg = new HostGraph();
+    hg->n = (uint32_t)V64;
+    hg->off.reserve(E64 + 1);
+    hg->off.push_back(0);
+    std::vector<uint32_t> nodes;
+    for (uint64_t i = 0; i < E64; ++i) {
+        if (!next_line(ls, le)) { delete hg; return AXC_EFORMAT; }  // unexpected end of file
+        q = ls;
+        float w = 1.0f;
+        if (edge_w) {
+            char tmp[64];
+            while (q < le && (*q == ' ' || *q == '\t')) ++q;
+            size_t k = 0;
+            while (q < le && *q != ' ' && *q != '\t' && k < 63) tmp[k++] = *q++;
+            tmp[k] = 0;
+            char *ep = nullptr;
+            w = std::strtof(tmp, &ep);
+            if (ep == tmp) { delete hg; return AXC_EFORMAT; }
+        }
+        nodes.clear();
+        uint64_t v;
+        while (parse_u64(q, le, v)) {
+            if (v == 0 || v > V64) { delete hg; return AXC_EFORMAT; }  // "Invalid node encountered"
+            nodes.push_back((uint32_t)(v - 1));
+        }
+        if (nodes.empty()) { delete hg; return AXC_EFORMAT; }
+        if (nodes.size() == 1) continue;  // singleton nets are skipped (hgraph.hpp:989-992)
+        hg->pins.insert(hg->pins.end(), nodes.begin(), nodes.end());
+        hg->nsrc.push_back(0);
+        hg->w.push_back(w);
+        hg->off.push_back(hg->pins.size());
+    }
+    publish(hg, out);
+    return AXC_OK;
+}
+
+extern "C" int axc_read_auto(const char *path, axc_hgraph *out) {
+    if (!path) return AXC_EINVAL;
+    std::string s(path);
+    auto ends = [&](const char *x) {
+        size_t l = std::strlen(x);
+        return s.size() >= l && s.compare(s.size() - l, l, x) == 0;
+    };
+    if (ends(".hgr")) return axc_read_hgr(path, out);
+    if (ends(".snn")) return axc_read_snn(path, out);
+    if (ends(".axh")) return axc_read_axh(path, out);
+    return AXC_EFORMAT;  // runconfig.cpp:171-173
+}
+
+static int write_snn(const char *path, const axc_hgraph *g) {
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return AXC_EIO;
+    std::vector<uint32_t> rec;
+    uint32_t hdr[2] = {g->n, g->e};
+    std::fwrite(hdr, 4, 2, f);
+    for (uint32_t i = 0; i < g->e; ++i) {
+        uint64_t a = g->hedge_off[i], b = g->hedge_off[i + 1];
+        uint32_t dstc = (uint32_t)(b - a - 1);  // saveSNN keeps the first pin as the source
+        std::fwrite(&dstc, 4, 1, f);
+        std::fwrite(g->pins + a, 4, (size_t)(b - a), f);
+        float w = g->hedge_w ? g->hedge_w[i] : 1.0f;
+        std::fwrite(&w, 4, 1, f);
+    }
+    return std::fclose(f) == 0 ? AXC_OK : AXC_EIO;
+}
+
+static int write_axh(const char *path, const axc_hgraph *g) {
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return AXC_EIO;
+    uint32_t hdr[2] = {g->n, g->e};
+    std::fwrite(hdr, 4, 2, f);
+    for (uint32_t i = 0; i < g->e; ++i) {
+        uint64_t a = g->hedge_off[i], b = g->hedge_off[i + 1];
+        uint32_t rec[2] = {(uint32_t)(b - a), g->src_count[i]};
+        if (rec[1] == 0 || rec[0] < rec[1]) { std::fclose(f); return AXC_EINVAL; }
+        std::fwrite(rec, 4, 2, f);
+        std::fwrite(g->pins + a, 4, (size_t)(b - a), f);
+        float w = g->hedge_w ? g->hedge_w[i] : 1.0f;
+        std::fwrite(&w, 4, 1, f);
+    }
+    return std::fclose(f) == 0 ? AXC_OK : AXC_EIO;
+}
+
+static int write_hgr(const char *path, const axc_hgraph *g) {
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return AXC_EIO;
+    bool emit_w = false;
+    for (uint32_t i = 0; g->hedge_w && i < g->e; ++i)
+        if (g->hedge_w[i] != 1.0f) { emit_w = true; break; }
+    std::fprintf(f, emit_w ? "%u %u 01\n" : "%u %u\n", g->e, g->n);
+    std::string line;
+    char tmp[32];
+    for (uint32_t i = 0; i < g->e; ++i) {
+        line.clear();
+        if (emit_w) {
+            // savehMETIS writes uint32(w * 1024) (hgraph.hpp:1040)
+            std::snprintf(tmp, sizeof tmp, "%u ", (uint32_t)(g->hedge_w[i] * 1024.0f));
+            line += tmp;
+        }
+        for (uint64_t k = g->hedge_off[i]; k < g->hedge_off[i + 1]; ++k) {
+            std::snprintf(tmp, sizeof tmp, k + 1 < g->hedge_off[i + 1] ? "%u " : "%u", g->pins[k] + 1);
+            line += tmp;
+        }
+        line += '\n';
+        std::fwrite(line.data(), 1, line.size(), f);
+    }
+    return std::fclose(f) == 0 ? AXC_OK : AXC_EIO;
+}
+
+extern "C" int axc_write_hgraph(const char *path, const axc_hgraph *g) {
+    if (!path || !g) return AXC_EINVAL;
+    std::string s(path);
+    auto ends = [&](const char *x) {
+        size_t l = std::strlen(x);
+        return s.size() >= l && s.compare(s.size() - l, l, x) == 0;
+    };
+    if (ends(".snn")) return write_snn(path, g);
+    if (ends(".axh")) return write_axh(path, g);
+    if (ends(".hgr")) return write_hgr(path, g);
+    return AXC_EFORMAT;
+}
+
+extern "C" int axc_write_partition(const char *path, const uint32_t *part, uint32_t n) {
+    if (!path || (!part && n)) return AXC_EINVAL;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return AXC_EIO;
+    std::string out;
+    out.reserve((size_t)n * 7);
+    char tmp[16];
+    for (uint32_t i = 0; i < n; ++i) {
+        int l = std::snprintf(tmp, sizeof tmp, "%u\n", part[i]);
+        out.append(tmp, (size_t)l);
+    }
+    size_t w = std::fwrite(out.data(), 1, out.size(), f);
+    int rc = std::fclose(f);
+    return (w == out.size() && rc == 0) ? AXC_OK : AXC_EIO;
+}
+
+extern "C" int axc_read_partition(const char *path, uint32_t n, uint32_t *out) {
+    if (!path || (!out && n)) return AXC_EINVAL;
+    std::vector<char> buf;
+    if (!read_file(path, buf)) return AXC_EIO;
+    buf.push_back('\n');
+    const char *p = buf.data(), *end = p + buf.size() - 1;
+    uint32_t idx = 0;
+    while (p < end) {
+        const char *e = (const char *)std::memchr(p, '\n', (size_t)(end + 1 - p));
+        const char *q = p, *le = e;
+        if (le > q && le[-1] == '\r') --le;
+        while (q < le && (*q == ' ' || *q == '\t')) ++q;
+        if (idx >= n) return AXC_EFORMAT;  // more entries than nodes (hgraph.hpp:1070)
+        uint64_t v = 0;
+        if (q >= le || *q < '0' || *q > '9') return AXC_EFORMAT;
+        while (q < le && *q >= '0' && *q <= '9') {
+            v = v * 10 + (uint64_t)(*q - '0');
+            if (v > 0xFFFFFFFFull) return AXC_EFORMAT;
+            ++q;
+        }
+        while (q < le && (*q == ' ' || *q == '\t')) ++q;
+        if (q != le) return AXC_EFORMAT;  // trailing data (hgraph.hpp:1075)
+        out[idx++] = (uint32_t)v;
+        p = e + 1;
+    }
+    return idx == n ? AXC_OK : AXC_EFORMAT;
+}
+
+// Quotient hypergraph of getPartitionsHypergraph(part, remove_self_cycles=2, squish=true)
+// (includes/hgraph.hpp:286-376): per hedge the distinct source partitions and the distinct
+// destination partitions minus the source ones; hedges with <= 1 source partition and no
+// destination partition vanish; identical (sources, destinations) pairs merge with summed weight.
+// The reference merges by a 64-bit hash of the pair; this version merges by the exact pair and
+// emits hedges in ascending (sources, destinations) order.
+extern "C" int axc_quotient_hgraph(const axc_hgraph *g, const uint32_t *part, axc_hgraph *out) {
+    if (!g || !part || !out) return AXC_EINVAL;
+    uint32_t K = 0;
+    for (uint32_t v = 0; v < g->n; ++v) K = std::max(K, part[v] + 1);
+    std::map<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>, double> acc;
+    std::vector<uint32_t> sp, dp;
+    for (uint32_t i = 0; i < g->e; ++i) {
+        uint64_t a = g->hedge_off[i], b = g->hedge_off[i + 1];
+        sp.clear(); dp.clear();
+        for (uint64_t k = a; k < b; ++k) {
+            uint32_t pp = part[g->pins[k]];
+            if (k < a + g->src_count[i]) sp.push_back(pp); else dp.push_back(pp);
+        }
+        std::sort(sp.begin(), sp.end()); sp.erase(std::unique(sp.begin(), sp.end()), sp.end());
+        std::sort(dp.begin(), dp.end()); dp.erase(std::unique(dp.begin(), dp.end()), dp.end());
+        std::vector<uint32_t> d2;
+        std::set_difference(dp.begin(), dp.end(), sp.begin(), sp.end(), std::back_inserter(d2));
+        if (sp.size() <= 1 && d2.empty()) continue;
+        acc[{sp, d2}] += g->hedge_w ? (double)g->hedge_w[i] : 1.0;
+    }
+    auto *hg = new HostGraph();
+    hg->n = K;
+    hg->off.push_back(0);
+    for (auto &kv : acc) {
+        hg->pins.insert(hg->pins.end(), kv.first.first.begin(), kv.first.first.end());
+        hg->pins.insert(hg->pins.end(), kv.first.second.begin(), kv.first.second.end());
+        hg->nsrc.push_back((uint32_t)kv.first.first.size());
+        hg->w.push_back((float)kv.second);
+        hg->off.push_back(hg->pins.size());
+    }
+    publish(hg, out);
+    return AXC_OK;
+}

@@ -1,0 +1,336 @@
+// Device primitives owned by the library (no Thrust/CUB): exclusive scans (reduce-then-scan over
+// 2048-element tiles), a stable LSD radix sort with warp-level match_any ranking, stable index
+// compaction, fills and reductions. Every launch goes through the context's stream.
+#include "common.cuh"
+
+namespace axc {
+
+namespace {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <class T>
+__device__ __forceinline__ T block_excl_scan(T v, T *warp_tot, T &block_total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        T t = lane < (blockDim.x >> 5) ? warp_tot[lane] : T(0);
+        T s = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < (blockDim.x >> 5)) warp_tot[lane] = s - t;
+        if (lane == (int)(blockDim.x >> 5) - 1) warp_tot[32] = s;
+    }
+    __syncthreads();
+    T r = x - v + warp_tot[w];
+    block_total = warp_tot[32];
+    __syncthreads();
+    return r;
+}
+
+template <class TI, class TO>
+__global__ void k_tile_reduce(const TI *__restrict__ in, TO *__restrict__ part, u64 n) {
+    __shared__ TO wt[33];
+    const u64 base = (u64)blockIdx.x * SCAN_TILE;
+    TO s = 0;
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        u64 i = base + (u64)j * SCAN_THREADS + threadIdx.x;
+        if (i < n) s += (TO)in[i];
+    }
+    TO tot;
+    block_excl_scan<TO>(s, wt, tot);
+    if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+template <class TI, class TO>
+__global__ void k_tile_scan(const TI *__restrict__ in, TO *__restrict__ out, const TO *__restrict__ part,
+                            u64 n) {
+    __shared__ TO wt[33];
+    __shared__ TO stage[SCAN_TILE + SCAN_TILE / 32];
+    const u64 base = (u64)blockIdx.x * SCAN_TILE;
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = j * SCAN_THREADS + threadIdx.x;
+        u64 i = base + li;
+        stage[li + li / 32] = i < n ? (TO)in[i] : TO(0);
+    }
+    __syncthreads();
+    TO loc[SCAN_ITEMS];
+    TO s = 0;
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = threadIdx.x * SCAN_ITEMS + j;
+        loc[j] = stage[li + li / 32];
+        s += loc[j];
+    }
+    TO tot;
+    TO pre = block_excl_scan<TO>(s, wt, tot) + (part ? part[blockIdx.x] : TO(0));
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = threadIdx.x * SCAN_ITEMS + j;
+        stage[li + li / 32] = pre;
+        pre += loc[j];
+    }
+    __syncthreads();
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = j * SCAN_THREADS + threadIdx.x;
+        u64 i = base + li;
+        if (i < n) out[i] = stage[li + li / 32];
+    }
+}
+
+template <class TI, class TO>
+void scan_impl(Ctx &c, const TI *in, TO *out, u64 n) {
+    if (n == 0) return;
+    const u32 tiles = cdiv(n, SCAN_TILE);
+    if (tiles == 1) {
+        LAUNCH(c, (k_tile_scan<TI, TO>), 1, SCAN_THREADS, 0, in, out, (const TO *)nullptr, n);
+        return;
+    }
+    size_t m = c.arena.mark();
+    TO *part = c.arena.alloc<TO>(tiles);
+    LAUNCH(c, (k_tile_reduce<TI, TO>), tiles, SCAN_THREADS, 0, in, part, n);
+    scan_impl<TO, TO>(c, part, part, tiles);
+    LAUNCH(c, (k_tile_scan<TI, TO>), tiles, SCAN_THREADS, 0, in, out, (const TO *)part, n);
+    c.arena.release(m);
+}
+
+__global__ void k_offsets_tail(const u32 *counts, u64 *out, u64 n) {
+    out[n] = (n ? out[n - 1] + counts[n - 1] : 0);
+}
+
+// ------------------------------------------------------------------ radix sort
+constexpr int RS_WARPS = 8;
+constexpr int RS_ITEMS = 8;  // rounds of 32 per warp
+constexpr int RS_TILE = RS_WARPS * 32 * RS_ITEMS;
+
+__global__ void k_rs_hist(const u32 *__restrict__ keys, u64 n, u32 shift, u32 *__restrict__ hist,
+                          u32 tiles) {
+    __shared__ u32 cnt[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const u64 base = (u64)blockIdx.x * RS_TILE;
+    for (int j = threadIdx.x; j < RS_TILE; j += blockDim.x) {
+        u64 i = base + j;
+        if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[(u64)d * tiles + blockIdx.x] = cnt[d];
+}
+
+__global__ void k_rs_scatter(const u32 *__restrict__ kin, const u32 *__restrict__ vin, u32 *__restrict__ kout,
+                             u32 *__restrict__ vout, u64 n, u32 shift, const u32 *__restrict__ offs,
+                             u32 tiles) {
+    __shared__ u32 wcnt[RS_WARPS][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < RS_WARPS * 256; i += blockDim.x) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const u64 base = (u64)blockIdx.x * RS_TILE + (u64)w * 32 * RS_ITEMS;
+    u32 dig[RS_ITEMS], loc[RS_ITEMS], key[RS_ITEMS], val[RS_ITEMS];
+    const u32 lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; ++r) {
+        u64 i = base + (u64)r * 32 + lane;
+        bool ok = i < n;
+        key[r] = ok ? kin[i] : 0u;
+        val[r] = ok ? vin[i] : 0u;
+        u32 d = ok ? ((key[r] >> shift) & 255u) : 256u;
+        dig[r] = d;
+        u32 peers = __match_any_sync(0xFFFFFFFFu, d);
+        u32 before = ok ? wcnt[w][d] : 0u;
+        loc[r] = before + __popc(peers & lt);
+        __syncwarp();
+        if (ok && (peers & lt) == 0) wcnt[w][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) {
+        u32 run = offs[(u64)d * tiles + blockIdx.x];
+        for (int ww = 0; ww < RS_WARPS; ++ww) {
+            u32 t = wcnt[ww][d];
+            wcnt[ww][d] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; ++r) {
+        if (dig[r] < 256u) {
+            u32 pos = wcnt[w][dig[r]] + loc[r];
+            kout[pos] = key[r];
+            vout[pos] = val[r];
+        }
+    }
+}
+
+__global__ void k_fill_u32(u32 *p, u32 v, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_iota_u32(u32 *p, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) p[i] = (u32)i;
+}
+__global__ void k_gather_u32(const u32 *src, const u32 *idx, u32 *dst, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+__global__ void k_reduce_sum(const u32 *p, u64 n, unsigned long long *out) {
+    u64 s = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) s += p[i];
+    s = warp_sum<u64>(s);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)s);
+}
+__global__ void k_reduce_max(const u32 *p, u64 n, u32 *out) {
+    u32 m = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        m = max(m, p[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+__global__ void k_reduce_sum64(const u64 *p, u64 n, unsigned long long *out) {
+    u64 s = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) s += p[i];
+    s = warp_sum<u64>(s);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)s);
+}
+__global__ void k_reduce_max64(const u64 *p, u64 n, unsigned long long *out) {
+    u64 m = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        m = p[i] > m ? p[i] : m;
+    m = warp_max_u64(m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)m);
+}
+__global__ void k_flag_to_u32(const u32 *flags, u32 *f01, u64 n) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        f01[i] = flags[i] ? 1u : 0u;
+}
+__global__ void k_compact_write(const u32 *flags, const u32 *pos, u32 *out, u64 n, u32 *total) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        if (flags[i]) out[pos[i]] = (u32)i;
+        if (i == n - 1) *total = pos[i] + (flags[i] ? 1u : 0u);
+    }
+}
+
+inline u32 grid_for(Ctx &c, u64 n, u32 threads = 256) {
+    u64 b = (n + threads - 1) / threads;
+    u64 cap = (u64)c.sms * 8;
+    return (u32)(b < cap ? (b ? b : 1) : cap);
+}
+
+}  // namespace
+
+void scan_excl_u32(Ctx &c, const u32 *in, u32 *out, u64 n) { scan_impl<u32, u32>(c, in, out, n); }
+void scan_excl_u64(Ctx &c, const u64 *in, u64 *out, u64 n) { scan_impl<u64, u64>(c, in, out, n); }
+void scan_excl_i64(Ctx &c, const i64 *in, i64 *out, u64 n) { scan_impl<i64, i64>(c, in, out, n); }
+
+void offsets_from_counts(Ctx &c, const u32 *counts, u64 *out, u64 n) {
+    if (n) scan_impl<u32, u64>(c, counts, out, n);
+    LAUNCH(c, k_offsets_tail, 1, 1, 0, counts, out, n);
+}
+
+void fill_u32(Ctx &c, u32 *p, u32 v, u64 n) {
+    if (n) LAUNCH(c, k_fill_u32, grid_for(c, n), 256, 0, p, v, n);
+}
+void iota_u32(Ctx &c, u32 *p, u64 n) {
+    if (n) LAUNCH(c, k_iota_u32, grid_for(c, n), 256, 0, p, n);
+}
+
+u64 reduce_sum_u32(Ctx &c, const u32 *p, u64 n) {
+    size_t m = c.arena.mark();
+    unsigned long long *d = c.arena.alloc<unsigned long long>(1);
+    AXC_CUDA(cudaMemsetAsync(d, 0, 8, c.stream));
+    if (n) LAUNCH(c, k_reduce_sum, grid_for(c, n), 256, 0, p, n, d);
+    u64 r = fetch1(c, (const u64 *)d);
+    c.arena.release(m);
+    return r;
+}
+u32 reduce_max_u32(Ctx &c, const u32 *p, u64 n) {
+    size_t m = c.arena.mark();
+    u32 *d = c.arena.alloc<u32>(1);
+    AXC_CUDA(cudaMemsetAsync(d, 0, 4, c.stream));
+    if (n) LAUNCH(c, k_reduce_max, grid_for(c, n), 256, 0, p, n, d);
+    u32 r = fetch1(c, d);
+    c.arena.release(m);
+    return r;
+}
+
+u64 reduce_sum_u64(Ctx &c, const u64 *p, u64 n) {
+    size_t m = c.arena.mark();
+    unsigned long long *d = c.arena.alloc<unsigned long long>(1);
+    AXC_CUDA(cudaMemsetAsync(d, 0, 8, c.stream));
+    if (n) LAUNCH(c, k_reduce_sum64, grid_for(c, n), 256, 0, p, n, d);
+    u64 r = fetch1(c, (const u64 *)d);
+    c.arena.release(m);
+    return r;
+}
+u64 reduce_max_u64(Ctx &c, const u64 *p, u64 n) {
+    size_t m = c.arena.mark();
+    unsigned long long *d = c.arena.alloc<unsigned long long>(1);
+    AXC_CUDA(cudaMemsetAsync(d, 0, 8, c.stream));
+    if (n) LAUNCH(c, k_reduce_max64, grid_for(c, n), 256, 0, p, n, d);
+    u64 r = fetch1(c, (const u64 *)d);
+    c.arena.release(m);
+    return r;
+}
+
+u32 compact_indices(Ctx &c, const u32 *flags, u32 *out, u64 n) {
+    if (n == 0) return 0;
+    size_t m = c.arena.mark();
+    u32 *f01 = c.arena.alloc<u32>(n);
+    u32 *pos = c.arena.alloc<u32>(n);
+    u32 *tot = c.arena.alloc<u32>(1);
+    LAUNCH(c, k_flag_to_u32, grid_for(c, n), 256, 0, flags, f01, n);
+    scan_excl_u32(c, f01, pos, n);
+    LAUNCH(c, k_compact_write, grid_for(c, n), 256, 0, flags, pos, out, n, tot);
+    u32 r = fetch1(c, tot);
+    c.arena.release(m);
+    return r;
+}
+
+void radix_sort_pairs(Ctx &c, u32 *keys, u32 *vals, u64 n, u32 bits) {
+    if (n <= 1 || bits == 0) return;
+    size_t m = c.arena.mark();
+    const u32 tiles = cdiv(n, RS_TILE);
+    u32 *k2 = c.arena.alloc<u32>(n), *v2 = c.arena.alloc<u32>(n);
+    u32 *hist = c.arena.alloc<u32>((u64)tiles * 256);
+    u32 *ka = keys, *va = vals, *kb = k2, *vb = v2;
+    for (u32 shift = 0; shift < bits; shift += 8) {
+        LAUNCH(c, k_rs_hist, tiles, 256, 0, ka, n, shift, hist, tiles);
+        scan_excl_u32(c, hist, hist, (u64)tiles * 256);
+        LAUNCH(c, k_rs_scatter, tiles, RS_WARPS * 32, 0, ka, va, kb, vb, n, shift, hist, tiles);
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    if (ka != keys) {
+        AXC_CUDA(cudaMemcpyAsync(keys, ka, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+        AXC_CUDA(cudaMemcpyAsync(vals, va, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    c.arena.release(m);
+}
+
+void radix_sort_pairs64(Ctx &c, u32 *key_hi, u32 *key_lo, u32 *vals, u64 n, u32 bits_hi, u32 bits_lo) {
+    if (n <= 1) return;
+    size_t m = c.arena.mark();
+    u32 *idx = c.arena.alloc<u32>(n), *tmp = c.arena.alloc<u32>(n);
+    iota_u32(c, idx, n);
+    radix_sort_pairs(c, key_lo, idx, n, bits_lo);           // idx: order by lo
+    LAUNCH(c, k_gather_u32, grid_for(c, n), 256, 0, key_hi, idx, tmp, n);  // hi in that order
+    radix_sort_pairs(c, tmp, idx, n, bits_hi);              // stable by hi
+    LAUNCH(c, k_gather_u32, grid_for(c, n), 256, 0, vals, idx, key_lo, n);  // reuse key_lo as scratch
+    AXC_CUDA(cudaMemcpyAsync(vals, key_lo, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    AXC_CUDA(cudaMemcpyAsync(key_hi, tmp, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    c.arena.release(m);
+}
+
+}  // namespace axc

@@ -1,0 +1,330 @@
+"""Benchmark: pins/s of the whole multilevel partitioner (end to end, at the reference's metric).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+A step partitions one seeded synthetic hypergraph of the named workload end to end:
+  value  pins/s with the raw hypergraph already resident in HBM (axc_partition_device), the L2
+         flushed between steps (outside the timed step);
+  e2e    pins/s through axc_partition with pinned host buffers: the upload of the step's input and
+         the download of its partition are inside the timed region.
+`--impl reference` times the reference's own implementation of the path on this box: its GPU
+build compiled from the reference sources (oracle/_ref/hgraph_gpu.exe, the span it reports as
+"Total host execution time"), or the CPU port of the oracle where the reference cannot run the
+mode (k-way needs the external Mt-KaHyPar binary).
+Multi-GPU (torchrun): one partition job does not shard, so every rank runs a replica; timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (description, reference CLI flags)
+    "snn-8x512": ("layered SNN 8x512 fan-out 64 seed 0, INCC omega=128 delta=1024 Kmax=1048576",
+                  ["-m", "128", "1024", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"]),
+    "circuit-200k-k2": ("circuit .hgr 200k nodes 220k nets seed 1, k-way k=2 eps=0.03",
+                        ["-k", "2", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
+    "circuit-200k-k64": ("circuit .hgr 200k nodes 220k nets seed 1, k-way k=64 eps=0.03",
+                         ["-k", "64", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
+    "snn-1m-incc": ("large SNN 20x50k lognormal fan-out seed 2, INCC omega=1024 delta=4096 Kmax=1048576",
+                    ["-m", "1024", "4096", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"]),
+    "snn-1m-k128": ("large SNN 20x50k lognormal fan-out seed 2, k-way k=128 eps=0.03",
+                    ["-k", "128", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
+}
+DEFAULT_WORKLOAD = "snn-8x512"
+METRIC = "pins/s end-to-end at equal lambda-1"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier_max(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def traffic_model(st) -> dict:
+    """Algorithmic bytes of the rating kernel per step (each node streams its incident hyperedges'
+    pins: 4 B per pin visit, plus 28 B per incidence entry for the touching list, offsets, weight
+    and source count)."""
+    visits = int(st.rating_pin_visits)
+    touch = sum(int(st.level_pins[i]) for i in range(min(int(st.levels), 64)))
+    return {"rating_bytes": 4 * visits + 28 * touch, "pin_visits": visits}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import axoncuda_b200 as ax
+    g, p = ax.workload(args.workload)
+    P = g.P
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = ax.Context(local, 0)
+    # ---- device-resident input (value) ----
+    d_off = torch.from_numpy(g.off.astype(np.uint64).view(np.int64)).to(dev)
+    d_pins = torch.from_numpy(g.pins.view(np.int32)).to(dev)
+    d_ns = torch.from_numpy(g.nsrc.view(np.int32)).to(dev)
+    d_w = torch.from_numpy(g.w).to(dev)
+    d_out = torch.empty(max(g.n, 1), dtype=torch.int32, device=dev)
+    import ctypes as C
+    dg = ax.HGraph(g.n, g.e, C.cast(d_off.data_ptr(), C.POINTER(C.c_uint64)),
+                   C.cast(d_pins.data_ptr(), C.POINTER(C.c_uint32)), C.cast(d_ns.data_ptr(), C.POINTER(C.c_uint32)),
+                   C.cast(d_w.data_ptr(), C.POINTER(C.c_float)), None)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    st = ax.Stats()
+
+    def dev_step():
+        rc = ax.lib().axc_partition_device(ctx._h, C.byref(dg), C.byref(p),
+                                           C.cast(d_out.data_ptr(), C.POINTER(C.c_uint32)), C.byref(st))
+        if rc:
+            raise ax.AxcError(rc, ax.lib().axc_last_error(ctx._h).decode())
+
+    for _ in range(args.warmup):
+        dev_step()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    launches = 0
+    rating_ms = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            barrier(world)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dev_step()
+            e1.record()
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            launches += int(st.kernel_launches)
+    total_ms = barrier_max(world, total_ms)
+    ms_step = total_ms / args.steps
+    value = world * P / (ms_step / 1e3)
+    # ---- end to end through the host-buffer C-ABI call (pinned buffers) ----
+    h_off = torch.from_numpy(g.off.view(np.int64)).pin_memory()
+    h_pins = torch.from_numpy(g.pins.view(np.int32)).pin_memory()
+    h_ns = torch.from_numpy(g.nsrc.view(np.int32)).pin_memory()
+    h_w = torch.from_numpy(g.w).pin_memory()
+    h_out = torch.empty(max(g.n, 1), dtype=torch.int32).pin_memory()
+    hg = ax.HGraph(g.n, g.e, C.cast(h_off.data_ptr(), C.POINTER(C.c_uint64)),
+                   C.cast(h_pins.data_ptr(), C.POINTER(C.c_uint32)), C.cast(h_ns.data_ptr(), C.POINTER(C.c_uint32)),
+                   C.cast(h_w.data_ptr(), C.POINTER(C.c_float)), None)
+    st2 = ax.Stats()
+
+    def e2e_step():
+        rc = ax.lib().axc_partition(ctx._h, C.byref(hg), C.byref(p),
+                                    C.cast(h_out.data_ptr(), C.POINTER(C.c_uint32)), C.byref(st2))
+        if rc:
+            raise ax.AxcError(rc, ax.lib().axc_last_error(ctx._h).decode())
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+    e2e_ms = barrier_max(world, e2e_ms)
+    e2e_step_ms = e2e_ms / args.steps
+    part = h_out.numpy()[: g.n].view(np.uint32).copy()
+    h2d = g.off.nbytes + g.pins.nbytes + g.nsrc.nbytes + g.w.nbytes
+    d2h = 4 * g.n
+    out = {
+        "metric": METRIC, "value": value, "unit": "pins/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload][0], "pins": P,
+                   "nodes": g.n, "hyperedges": g.e, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) between timed steps"},
+        "e2e": {"value": world * P / (e2e_step_ms / 1e3), "unit": "pins/s", "ms_per_step": e2e_step_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "quality": {"connectivity": st2.connectivity, "cutnet": st2.cutnet, "num_parts": int(st2.num_parts),
+                    "valid": int(st2.valid), "levels": int(st2.levels)},
+        "clocks": clk.summary(),
+    }
+    tm = traffic_model(st)
+    out["roofline"] = None
+    out["_traffic_model"] = tm
+    ctx.close()
+    return out, g, p, part
+
+
+def cpu_port_baseline(g, p, budget_s: float = 30.0) -> dict:
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    if p.mode == 0:
+        O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 0, omega=p.omega, delta=p.delta, max_parts=p.max_parts,
+                    cnc=p.cnc, rfr=p.rfr, ipm=p.ipm, seed=p.seed)
+    else:
+        O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 1, k=p.k, eps=p.eps, cnc=p.cnc, rfr=p.rfr, seed=p.seed)
+    dt = time.perf_counter() - t0
+    return {"value": g.P / dt, "unit": "pins/s", "cores": 1, "kind": "port",
+            "sample": f"one full step of the workload ({g.P} pins) through the oracle's single-threaded "
+                      f"C++ restatement of the whole partitioner, {dt:.2f} s"}
+
+
+def run_reference(args):
+    """The reference's own implementation of the path, timed on this box."""
+    import axoncuda_b200 as ax
+    g, p = ax.workload(args.workload)
+    exe = os.path.join(ROOT, "oracle", "_ref", "hgraph_gpu.exe")
+    flags = WORKLOADS[args.workload][1]
+    kway = p.mode == ax.MODE_KWAY
+    line = {"metric": METRIC, "unit": "pins/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][0], "pins": g.P}}
+    if not kway and os.path.exists(exe):
+        with tempfile.TemporaryDirectory() as td:
+            ext = ".hgr" if "circuit" in args.workload else ".snn"
+            path = os.path.join(td, "in" + ext)
+            ax.write(path, g)
+            times = []
+            conn = None
+            for i in range(args.warmup + args.steps):
+                pf = os.path.join(td, "out.part")
+                r = subprocess.run([exe, "-r", path, *flags, "-p", pf], capture_output=True, text=True, cwd=td)
+                if r.returncode != 0:
+                    line["unavailable"] = f"reference exited {r.returncode}: {r.stderr.strip()[-200:]}"
+                    return line
+                m = re.search(r"Total host execution time: ([0-9.]+) ms", r.stdout)
+                if i >= args.warmup:
+                    times.append(float(m.group(1)))
+                mc = re.search(r"Connectivity:\s+([0-9.]+)", r.stdout)
+                conn = float(mc.group(1)) if mc else None
+            ms = sum(times) / len(times)
+            v = g.P / (ms / 1e3)
+            line.update({"value": v, "ms_per_step": ms,
+                         "cpu_baseline": {"value": v, "unit": "pins/s", "cores": 0, "kind": "reference",
+                                          "sample": "full workload through the reference GPU build "
+                                                    "(hgraph_gpu.exe, sm_100a), its 'Total host execution time'"},
+                         "e2e": {"value": v, "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "quality": {"connectivity": conn}})
+            return line
+    # k-way: the reference needs the external Mt-KaHyPar binary (sources/init_part.cu:891-906), which
+    # is not installable offline; time the oracle's CPU port instead.
+    cb = cpu_port_baseline(g, p)
+    line.update({"value": cb["value"], "ms_per_step": g.P / cb["value"] * 1e3, "cpu_baseline": cb,
+                 "e2e": {"value": cb["value"], "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "note": "reference k-way needs mtkahypar (absent); CPU port of the oracle timed instead"})
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    world, rank, local = dist_setup(args)
+    out, g, p, part = run_ours(args, world, rank, local)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_port_baseline(g, p)
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

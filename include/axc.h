@@ -1,0 +1,237 @@
+/*
+ * axc.h — C ABI of the B200-native multilevel hypergraph partitioner.
+ *
+ * The reference (AxonCUDA) exposes no library: its surface is the `hgraph_gpu.exe` process
+ * (sources/main.cu:38-940, flags in sources/runconfig.cpp:25-46), the .hgr/.snn/.axh readers
+ * (includes/hgraph.hpp:707-1013), and the per-node partition file scored by grading/grade.cpp.
+ * Every entry point below replaces one piece of that surface; the comment on each names the
+ * reference code it stands in for. The drop-in CLI (`axc_hgraph_gpu`) is a thin C++ client of
+ * this header.
+ *
+ * Conventions
+ *  - Every call returns an axc_status; nothing exits or aborts (the reference calls exit()/abort(),
+ *    headers/utils.cuh:16-22, sources/runconfig.cpp:74-127).
+ *  - Plain pointers and sizes only. Unless a parameter says "device", buffers are host memory
+ *    owned by the caller. The context owns all device memory.
+ *  - Node ids are uint32 and 0-based; pins of one hyperedge are stored sources first
+ *    (includes/hgraph.hpp:31-77). Offsets are uint64.
+ *  - Hyperedge weights are float in files and in axc_hgraph; on the device they become exact
+ *    fixed point w_fx = floor(w * 2^18) (the reference's FIXED_POINT_SCALE, headers/defines.cuh:24),
+ *    and every gain, cut and inbound count is integer arithmetic on those.
+ *  - Results are deterministic for a given input, parameter set and seed.
+ */
+#ifndef AXC_H
+#define AXC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    AXC_OK = 0,
+    AXC_EINVAL = 1,        /* bad argument or parameter */
+    AXC_ENOMEM = 2,        /* device arena or host allocation exhausted */
+    AXC_ECUDA = 3,         /* a CUDA runtime call failed */
+    AXC_EIO = 4,           /* file cannot be opened / read / written */
+    AXC_EFORMAT = 5,       /* malformed input file */
+    AXC_EINFEASIBLE = 6,   /* the result violates the constraints (reference: "ERROR, invalid partitining") */
+    AXC_ETIMEDOUT = 7,     /* a bounded device wait or a poll timed out */
+    AXC_ENOTFOUND = 8,     /* unknown job id */
+    AXC_EBUSY = 9,         /* admission refused (memory budget) */
+    AXC_EINTERNAL = 10,    /* device-side invariant check failed (status word set by a kernel) */
+    AXC_EOVERFLOW = 11     /* a size exceeds the documented limit of the call */
+} axc_status;
+
+typedef enum { AXC_MODE_INCC = 0, AXC_MODE_KWAY = 1 } axc_mode;
+
+/* Hypergraph in the reference's HyperGraph layout (includes/hgraph.hpp:130-168):
+ * hedge i owns pins[hedge_off[i] .. hedge_off[i+1]); the first src_count[i] are sources. */
+typedef struct {
+    uint32_t n;                 /* nodes */
+    uint32_t e;                 /* hyperedges */
+    const uint64_t *hedge_off;  /* [e+1] */
+    const uint32_t *pins;       /* [hedge_off[e]] */
+    const uint32_t *src_count;  /* [e] */
+    const float *hedge_w;       /* [e], NULL means every weight is 1 */
+    void *_owner;               /* non-NULL when the arrays belong to the library (axc_read_*, axc_gen_*) */
+} axc_hgraph;
+
+/* Run parameters: the runconfig of includes/runconfig.hpp:26-45 plus the constraint triple of
+ * includes/constr.hpp:14-19. */
+typedef struct {
+    int mode;              /* axc_mode */
+    uint32_t omega;        /* INCC: max nodes per partition (-m 1st) */
+    uint32_t delta;        /* INCC: max distinct inbound hyperedges per partition (-m 2nd) */
+    uint32_t max_parts;    /* INCC: max number of partitions (-m 3rd) */
+    uint32_t k;            /* KWAY: number of parts (-k) */
+    float eps;             /* KWAY: imbalance (-k) */
+    uint32_t cnc;          /* candidates per node (-cnc), <= AXC_MAX_CANDIDATES */
+    uint32_t rfr;          /* refinement rounds per level (-rfr) */
+    uint32_t smh;          /* -smh: accepted for CLI compatibility; level hierarchies stay resident */
+    int ipm;               /* -ipm: greedily merge the coarsest groups (INCC) */
+    float om;              /* -om: accepted for CLI compatibility; no oversized buffers are used */
+    uint64_t seed;         /* tie-break / noise seed; same seed => same partition */
+    int verbose;           /* -v 0..3 */
+} axc_params;
+
+#define AXC_MAX_CANDIDATES 16u   /* headers/defines.cuh:49 */
+#define AXC_FIXED_POINT_SCALE 262144u
+
+typedef struct {
+    uint32_t num_parts;        /* K' after zero-basing */
+    uint32_t levels;           /* coarsening levels built */
+    uint64_t pins;             /* pins after rule-2 deduplication (sources included) */
+    int64_t connectivity_fx;   /* sum_e w_fx(e) * (lambda_e - 1), exact */
+    int64_t cutnet_fx;         /* sum_e w_fx(e) * [lambda_e > 1] */
+    int64_t soed_fx;           /* sum_e w_fx(e) * (lambda_e - 1) * |e| over the input pins */
+    double connectivity;       /* connectivity_fx / 2^18 */
+    double cutnet;
+    double soed;
+    uint32_t max_part_size;    /* largest partition (nodes) */
+    uint32_t max_part_inbound; /* largest distinct-inbound count over partitions */
+    int valid;                 /* 1 iff checkPartitionValidity would accept (sources/constr.cpp:90-147) */
+    double ms_device;          /* device time from upload start to partition download end */
+    double ms_core;            /* device time of the multilevel core (after construction) */
+    uint32_t kernel_launches;  /* kernels this call launched */
+    uint64_t level_pins[64];   /* pins per level (for the traffic model) */
+    uint32_t level_nodes[64];
+    uint32_t refine_rounds[64];
+    uint64_t rating_pin_visits;  /* sum over rated nodes of incident pins visited */
+} axc_stats;
+
+typedef struct axc_ctx axc_ctx;
+
+/* ---- context --------------------------------------------------------------------------------
+ * One per device; owns a device arena of `arena_bytes` (0 = a default sized from free memory),
+ * one stream and the kernels' status word. Replaces the per-step cudaMalloc/cudaFree of
+ * sources/main.cu:196-222 and the host wrappers of sources/construction.cu, coarsening.cu,
+ * refinement.cu and postprocess.cu. */
+int axc_create(int device, size_t arena_bytes, axc_ctx **out);
+void axc_destroy(axc_ctx *ctx);
+const char *axc_strerror(int status);
+const char *axc_last_error(axc_ctx *ctx);   /* human-readable detail of the last failure */
+
+/* Defaults of sources/runconfig.cpp:48-70 (cnc=16, rfr=16, smh=2, om=1.5) with the given mode. */
+void axc_params_default(axc_params *p, int mode);
+/* Preset constraints of sources/constr.cpp:195-229: "loihi64", "loihi84", "loihi1024", "truenorth". */
+int axc_params_preset(axc_params *p, const char *name);
+/* KWAY constraint derivation of sources/runconfig.cpp:186-194: omega = ceil((1+eps)*n/k). */
+uint32_t axc_kway_omega(uint32_t n, uint32_t k, float eps);
+
+/* ---- the hot path -----------------------------------------------------------------------------
+ * Partition a host hypergraph end to end on the context's device: upload, rule-2 dedupe,
+ * incidence CSR, multilevel coarsening, initial partition, uncoarsening with refinement,
+ * INCC small-partition merge, zero-basing, download. Replaces main() from the upload at
+ * sources/main.cu:196 to the partition download at sources/main.cu:833-834 (the span the
+ * reference times as "Total host execution time", sources/main.cu:151-910).
+ * out_part: [g->n] host buffer. stats may be NULL. */
+int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32_t *out_part,
+                  axc_stats *stats);
+
+/* Same, with the hypergraph already resident in device memory (arrays are device pointers;
+ * hedge_w may be NULL) and the partition written to device memory d_out_part[n]. */
+int axc_partition_device(axc_ctx *ctx, const axc_hgraph *d_g, const axc_params *p,
+                         uint32_t *d_out_part, axc_stats *stats);
+
+/* ---- validity and metrics on the device --------------------------------------------------------
+ * Replaces Constraints::checkPartitionValidity (sources/constr.cpp:90-147) and the metrics of
+ * includes/hgraph.hpp:214-280 as printed by sources/main.cu:917-928 and grading/grade.cpp:298-309.
+ * `part` is host memory [g->n]. The hypergraph is used as given (no dedupe), like grade.cpp. */
+int axc_evaluate(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, const uint32_t *part,
+                 axc_stats *stats);
+
+/* ---- readers / writers (host) -------------------------------------------------------------------
+ * HyperGraph::loadhMETIS/loadSNN/loadAXH (includes/hgraph.hpp:936-1013, 707-743, 805-854) and
+ * loadHgraph's dispatch by extension (sources/runconfig.cpp:153-184). */
+int axc_read_hgr(const char *path, axc_hgraph *out);
+int axc_read_snn(const char *path, axc_hgraph *out);
+int axc_read_axh(const char *path, axc_hgraph *out);
+int axc_read_auto(const char *path, axc_hgraph *out);
+void axc_free_hgraph(axc_hgraph *g);
+/* saveSNN / saveAXH / savehMETIS (includes/hgraph.hpp:746-774, 856-883, 1016-1051). */
+int axc_write_hgraph(const char *path, const axc_hgraph *g);
+/* HyperGraph::savePartitioning (includes/hgraph.hpp:1054-1059): one decimal id per line. */
+int axc_write_partition(const char *path, const uint32_t *part, uint32_t n);
+/* HyperGraph::loadPartitioning (includes/hgraph.hpp:1062-1083). out: [n]. */
+int axc_read_partition(const char *path, uint32_t n, uint32_t *out);
+/* getPartitionsHypergraph(part, 2, squish=true) (includes/hgraph.hpp:286-376): the quotient
+ * hypergraph written by `-s`; identical (source set, destination set) hyperedges are merged. */
+int axc_quotient_hgraph(const axc_hgraph *g, const uint32_t *part, axc_hgraph *out);
+
+/* ---- synthetic inputs (seeded; stand-ins for the public SNN / ISPD suites) -----------------------
+ * Layered SNN: `layers` x `width` neurons; every neuron of layers 0..layers-2 owns one hyperedge
+ * (source = itself). Fan-out: fixed `fanout` when sigma <= 0, else lognormal(median=fanout, sigma)
+ * capped at `cap`. Each destination comes from the next layer with probability p_next, else
+ * uniformly from any later layer; drawn without replacement. Weights 1. */
+int axc_gen_snn(uint32_t layers, uint32_t width, double fanout, double sigma, uint32_t cap,
+                double p_next, uint64_t seed, axc_hgraph *out);
+/* Circuit-style netlist: n nodes, e nets, net sizes ~ s^-alpha on [smin, smax]; each pin is,
+ * with probability p_local, uniform within +-local_frac*n of a random anchor, else uniform;
+ * pins of one net are distinct. No sources (hMETIS nets). Weights 1. */
+int axc_gen_circuit(uint32_t n, uint32_t e, uint32_t smin, uint32_t smax, double alpha,
+                    double p_local, double local_frac, uint64_t seed, axc_hgraph *out);
+
+/* ---- batching and serving -------------------------------------------------------------------------
+ * Many independent jobs on one device. Jobs are uploaded, coarsened, partitioned and refined
+ * with their level hierarchies resident in the context's arena; job-level work of concurrent jobs
+ * overlaps on the device. Admission is by device-memory budget. There is no reference counterpart:
+ * the reference partitions exactly one hypergraph per process (sources/main.cu:38). */
+int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint64_t *job_id);
+/* Wait up to timeout_ms (<0: forever) for a job; copies its partition into out_part[n]. */
+int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms);
+/* Partition `count` jobs as one batch (one launch sequence shared by all jobs). out_parts[i]
+ * points at a host buffer of g[i].n entries. */
+int axc_partition_batch(axc_ctx *ctx, uint32_t count, const axc_hgraph *g, const axc_params *p,
+                        uint32_t *const *out_parts, axc_stats *stats);
+
+/* ---- stage entry points (host buffers in and out; for parity tests against the oracle) -----------
+ * Each runs exactly one stage of the device pipeline on the given level graph. */
+
+/* Rule-2 dedupe (includes/hgraph.hpp:518-581, rule 2: a destination equal to a source is dropped)
+ * followed by the per-node incidence CSR with inbound hyperedges first, each part ascending
+ * (sources/construction.cu:17-62, -dtc path kernels/construction.cu:9-84).
+ * out_hedge_off[e+1], out_pins[P], out_src_count[e]; out_touch_off[n+1], out_touch[P],
+ * out_inbound[n]. *out_pins_after receives the deduplicated pin count. */
+int axc_stage_construct(axc_ctx *ctx, const axc_hgraph *g, uint64_t *out_hedge_off,
+                        uint32_t *out_pins, uint32_t *out_src_count, uint64_t *out_touch_off,
+                        uint32_t *out_touch, uint32_t *out_inbound, uint64_t *out_pins_after);
+
+/* Candidate rating of kernels/coarsening.cu:10-213 on an already-deduplicated level graph with
+ * node sizes `node_size[n]`: top-`cnc` neighbors by (score desc, id desc), score = symmetric noise
+ * + sum over shared hyperedges of floor(w_fx/|e|); pairs violating omega or delta are dropped.
+ * out_pairs[n*cnc] (UINT32_MAX = none), out_scores[n*cnc]. */
+int axc_stage_rating(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *node_size, uint32_t omega,
+                     uint32_t delta, uint32_t cnc, uint64_t seed, uint32_t *out_pairs,
+                     uint32_t *out_scores);
+
+/* Matching over candidate lists plus orphan pairing (sources/coarsening.cu:70-210,
+ * sources/chaining.cu:260-329): out_groups[n] zero-based group ids ordered by their smallest
+ * member; *out_num_groups. */
+int axc_stage_matching(axc_ctx *ctx, uint32_t n, uint32_t cnc, const uint32_t *pairs,
+                       const uint32_t *scores, const uint32_t *node_size, const uint32_t *inbound,
+                       uint32_t omega, uint32_t delta, uint32_t *out_groups,
+                       uint32_t *out_num_groups);
+
+/* Contraction of hyperedges by a group map (kernels/construction.cu:304-489): coarse pins are the
+ * distinct groups, destinations win over sources, each part ascending, hyperedge count unchanged.
+ * out_hedge_off[e+1], out_pins[<= P], out_src_count[e]; *out_pins_after. */
+int axc_stage_contract(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *groups,
+                       uint32_t num_groups, uint64_t *out_hedge_off, uint32_t *out_pins,
+                       uint32_t *out_src_count, uint64_t *out_pins_after);
+
+/* Move gains of one refinement round for a given partition (kernels/refinement.cu:82-209 with
+ * exact integer arithmetic): for every node its best feasible target and isolated gain.
+ * part[n], part_size[K] (node-size sums), node_size[n]. encourage=1 selects the INCC saving
+ * sum floor(w_fx / c^2); 0 the k-way saving sum w_fx*[c == 1]. out_target[n] (UINT32_MAX = no
+ * move), out_gain[n]. */
+int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uint32_t num_parts,
+                    const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage,
+                    uint32_t discount, uint32_t *out_target, int64_t *out_gain);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AXC_H */

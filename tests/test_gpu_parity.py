@@ -1,0 +1,228 @@
+"""GPU parity: every stage of the device pipeline, called through the C ABI, against the oracle.
+
+Integer and index work must be bit-exact; the whole partitioner must return exactly the oracle's
+partition (same algorithm, same integer arithmetic, same tie-breaks) and pass the constraint check.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import axoncuda_b200 as ax
+from conftest import GOLDEN, GOLDEN_INPUTS
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+NONE = 0xFFFFFFFF
+
+
+def golden(name):
+    return ax.read(os.path.join(GOLDEN, name))
+
+
+def dedup(g):
+    off, pins, ns = O.dedupe(g.off, g.pins, g.nsrc)
+    return ax.Hypergraph(g.n, off, pins, ns, g.w.copy())
+
+
+@pytest.mark.parametrize("name", GOLDEN_INPUTS)
+def test_construct_matches_oracle(ctx, name):
+    g = golden(name)
+    off, pins, ns, toff, touch, nin = ctx.stage_construct(g)
+    o_off, o_pins, o_ns = O.dedupe(g.off, g.pins, g.nsrc)
+    np.testing.assert_array_equal(off, o_off)
+    np.testing.assert_array_equal(pins, o_pins)
+    np.testing.assert_array_equal(ns, o_ns)
+    t_off, t_touch, t_nin = O.touching(g.n, o_off, o_pins, o_ns)
+    np.testing.assert_array_equal(toff, t_off)
+    np.testing.assert_array_equal(touch, t_touch)
+    np.testing.assert_array_equal(nin, t_nin)
+
+
+@pytest.mark.parametrize("wl", ["snn-8x512", "circuit-200k-k2"])
+def test_construct_full_size(ctx, wl):
+    g, _ = ax.workload(wl)
+    off, pins, ns, toff, touch, nin = ctx.stage_construct(g)
+    o_off, o_pins, o_ns = O.dedupe(g.off, g.pins, g.nsrc)
+    np.testing.assert_array_equal(pins, o_pins)
+    t_off, t_touch, t_nin = O.touching(g.n, o_off, o_pins, o_ns)
+    np.testing.assert_array_equal(toff, t_off)
+    np.testing.assert_array_equal(touch, t_touch)
+    np.testing.assert_array_equal(nin, t_nin)
+
+
+def test_construct_with_duplicates_and_big_hyperedges(ctx):
+    # hyperedges of 300 and 9000 pins exercise the block and global-table paths
+    rng = np.random.default_rng(3)
+    sizes = [5, 300, 40, 9000, 2]
+    pins, off, ns = [], [0], []
+    for s in sizes:
+        v = rng.integers(0, 4000, s).astype(np.uint32)
+        v[s // 2:] = v[: s - s // 2]  # many duplicates
+        pins.append(v); off.append(off[-1] + s); ns.append(min(3, s - 1))
+    g = ax.Hypergraph(4000, np.array(off, np.uint64), np.concatenate(pins), np.array(ns, np.uint32),
+                      np.ones(len(sizes), np.float32))
+    off2, pins2, ns2, *_ = ctx.stage_construct(g)
+    o_off, o_pins, o_ns = O.dedupe(g.off, g.pins, g.nsrc)
+    np.testing.assert_array_equal(off2, o_off)
+    np.testing.assert_array_equal(pins2, o_pins)
+    np.testing.assert_array_equal(ns2, o_ns)
+
+
+RATING_CASES = [("snn_4x64.snn", 1, 1 << 20, 1 << 20, 4), ("snn_4x64.snn", 2, 3, 20, 8),
+                ("circ_2k.hgr", 1, 1 << 20, 1 << 20, 16), ("snn_5x40_ln.snn", 3, 7, 9, 4),
+                ("tiny_multi.axh", 1, 4, 4, 3), ("tiny_w.hgr", 1, 10, 10, 2)]
+
+
+@pytest.mark.parametrize("name,size,omega,delta,cnc", RATING_CASES)
+def test_rating_matches_oracle(ctx, name, size, omega, delta, cnc):
+    g = dedup(golden(name))
+    rng = np.random.default_rng(size)
+    ns = rng.integers(1, size + 1, g.n).astype(np.uint32)
+    pairs, scores = ctx.stage_rating(g, ns, omega, delta, cnc)
+    o_pairs, o_scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, omega, delta, cnc)
+    np.testing.assert_array_equal(pairs, o_pairs)
+    np.testing.assert_array_equal(scores, o_scores)
+
+
+@pytest.mark.parametrize("wl", ["snn-8x512", "circuit-200k-k2"])
+def test_rating_full_size(ctx, wl):
+    g, p = ax.workload(wl)
+    g = dedup(g)
+    ns = np.ones(g.n, np.uint32)
+    omega = p.omega if p.mode == 0 else 1 << 20
+    delta = p.delta if p.mode == 0 else 0x7FFFFFFF
+    pairs, scores = ctx.stage_rating(g, ns, omega, delta, 4)
+    o_pairs, o_scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, omega, delta, 4)
+    np.testing.assert_array_equal(pairs, o_pairs)
+    np.testing.assert_array_equal(scores, o_scores)
+
+
+@pytest.mark.parametrize("name,cnc", [("snn_4x64.snn", 4), ("circ_2k.hgr", 8), ("snn_5x40_ln.snn", 2)])
+def test_matching_matches_oracle(ctx, name, cnc):
+    g = dedup(golden(name))
+    ns = np.ones(g.n, np.uint32)
+    toff, touch, nin = O.touching(g.n, g.off, g.pins, g.nsrc)
+    pairs, _ = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 1 << 20, 1 << 20, cnc)
+    groups, ng = ctx.stage_matching(g.n, cnc, pairs, ns, nin, 1 << 20, 1 << 20)
+    o_groups, o_ng = O.matching(g.n, cnc, pairs, ns, nin, 1 << 20, 1 << 20)
+    assert ng == o_ng
+    np.testing.assert_array_equal(groups, o_groups)
+
+
+def test_matching_orphans(ctx):
+    # no candidates at all: everything is an orphan; pairing by (size, id) under omega and delta
+    n, cnc = 11, 2
+    pairs = np.full(n * cnc, NONE, np.uint32)
+    ns = np.array([3, 1, 4, 1, 5, 9, 2, 6, 5, 3, 5], np.uint32)
+    nin = np.array([1, 0, 2, 7, 1, 0, 3, 1, 2, 0, 1], np.uint32)
+    groups, ng = ctx.stage_matching(n, cnc, pairs, ns, nin, 10, 5)
+    o_groups, o_ng = O.matching(n, cnc, pairs, ns, nin, 10, 5)
+    assert ng == o_ng
+    np.testing.assert_array_equal(groups, o_groups)
+
+
+@pytest.mark.parametrize("name", GOLDEN_INPUTS)
+def test_contract_matches_oracle(ctx, name):
+    g = dedup(golden(name))
+    rng = np.random.default_rng(1)
+    ng = max(1, g.n // 2)
+    groups = rng.integers(0, ng, g.n).astype(np.uint32)
+    _, groups = np.unique(groups, return_inverse=True)
+    groups = groups.astype(np.uint32)
+    off, pins, ns = ctx.stage_contract(g, groups)
+    o_off, o_pins, o_ns = O.contract(g.off, g.pins, g.nsrc, groups)
+    np.testing.assert_array_equal(off, o_off)
+    np.testing.assert_array_equal(pins, o_pins)
+    np.testing.assert_array_equal(ns, o_ns)
+
+
+GAIN_CASES = [("snn_4x64.snn", 8, 1 << 20, 1 << 20, 1, 1), ("snn_4x64.snn", 8, 40, 60, 1, 2),
+              ("circ_2k.hgr", 4, 600, 0x7FFFFFFF, 0, 1), ("circ_2k.hgr", 17, 150, 0x7FFFFFFF, 0, 0xFFFFFFFF),
+              ("snn_5x40_ln.snn", 6, 50, 30, 1, 0xFFFFFFFF)]
+
+
+@pytest.mark.parametrize("name,K,omega,delta,enc,disc", GAIN_CASES)
+def test_gains_match_oracle(ctx, name, K, omega, delta, enc, disc):
+    g = dedup(golden(name))
+    rng = np.random.default_rng(K)
+    part = rng.integers(0, K, g.n).astype(np.uint32)
+    ns = rng.integers(1, 3, g.n).astype(np.uint32)
+    tgt, gain = ctx.stage_gains(g, part, K, ns, omega, delta, enc, disc)
+    o_tgt, o_gain = O.gains(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, part, K, omega, delta, enc, disc)
+    np.testing.assert_array_equal(tgt, o_tgt)
+    np.testing.assert_array_equal(gain, o_gain)
+
+
+def oracle_partition(g, p):
+    if p.mode == ax.MODE_INCC:
+        return O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 0, omega=p.omega, delta=p.delta,
+                           max_parts=p.max_parts, cnc=p.cnc, rfr=p.rfr, ipm=p.ipm, seed=p.seed)
+    return O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 1, k=p.k, eps=p.eps, cnc=p.cnc, rfr=p.rfr, seed=p.seed)
+
+
+E2E_SMALL = [("snn_4x64.snn", ax.params_incc(16, 64, 1 << 20, cnc=4, rfr=8)),
+             ("snn_4x64.snn", ax.params_kway(4, 0.05, cnc=4, rfr=8)),
+             ("circ_2k.hgr", ax.params_incc(50, 400, 1 << 20, cnc=8, rfr=16)),
+             ("circ_2k.hgr", ax.params_kway(8, 0.03, cnc=4, rfr=16)),
+             ("snn_5x40_ln.snn", ax.params_incc(12, 30, 1 << 20, cnc=2, rfr=6, ipm=0)),
+             ("tiny_multi.axh", ax.params_incc(3, 3, 1 << 20, cnc=2, rfr=4)),
+             ("tiny_dups.hgr", ax.params_kway(2, 0.5, cnc=2, rfr=4))]
+
+
+@pytest.mark.parametrize("i", range(len(E2E_SMALL)))
+def test_partition_matches_oracle(ctx, i):
+    name, p = E2E_SMALL[i]
+    g = golden(name)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.num_parts == o_K
+    assert st.valid == 1
+
+
+@pytest.mark.parametrize("wl", ["snn-8x512", "circuit-200k-k2"])
+def test_partition_full_size_matches_oracle(ctx, wl):
+    g, p = ax.workload(wl)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1
+    om = p.omega if p.mode == 0 else ax.kway_omega(g.n, p.k, p.eps)
+    de = p.delta if p.mode == 0 else 0x7FFFFFFF
+    kmax = p.max_parts if p.mode == 0 else p.k
+    ev = O.evaluate(g.n, g.off, g.pins, g.nsrc, g.w, part, om, de, kmax)
+    assert ev["valid"] == 1
+    assert ev["connectivity_fx"] == st.connectivity_fx
+
+
+def test_evaluate_matches_oracle(ctx):
+    g = golden("circ_2k.hgr")
+    rng = np.random.default_rng(5)
+    part = rng.integers(0, 9, g.n).astype(np.uint32)
+    _, part = np.unique(part, return_inverse=True)
+    part = part.astype(np.uint32)
+    p = ax.params_incc(300, 2000, 9)
+    st = ctx.evaluate(g, p, part)
+    ev = O.evaluate(g.n, g.off, g.pins, g.nsrc, g.w, part, 300, 2000, 9)
+    assert (st.connectivity_fx, st.cutnet_fx, st.soed_fx) == (ev["connectivity_fx"], ev["cutnet_fx"], ev["soed_fx"])
+    assert st.valid == ev["valid"] and st.num_parts == ev["num_parts"]
+    assert st.max_part_inbound == ev["max_inbound"]
+
+
+def test_same_seed_same_partition(ctx):
+    g, p = ax.workload("circuit-200k-k64")
+    a, _ = ctx.partition(g, p)
+    b, _ = ctx.partition(g, p)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_batch_queue_matches_solo(ctx):
+    jobs = [(ax.gen_circuit(3000 + 500 * i, 3300 + 500 * i, 2, 32, 2.5, 0.9, 0.02, 100 + i),
+             ax.params_kway([2, 8, 32][i % 3], 0.03, cnc=4, rfr=8)) for i in range(6)]
+    solo = [ctx.partition(g, p)[0] for g, p in jobs]
+    ids = [ctx.submit(g, p) for g, p in jobs]
+    for (g, _), jid, s in zip(jobs, ids, solo):
+        part, st = ctx.poll(jid, g.n)
+        np.testing.assert_array_equal(part, s)
+        assert st.valid == 1
