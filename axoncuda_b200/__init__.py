@@ -308,12 +308,13 @@ class Context:
                     "axc_stage_rating")
         return pairs[: n * cnc], scores[: n * cnc]
 
-    def stage_matching(self, n, cnc, pairs, node_size, inbound, omega, delta):
+    def stage_matching(self, n, cnc, pairs, scores, node_size, inbound, omega, delta):
         pairs = np.ascontiguousarray(pairs, dtype=np.uint32)
+        scores = np.ascontiguousarray(scores, dtype=np.uint32)
         ns = np.ascontiguousarray(node_size, dtype=np.uint32)
         nin = np.ascontiguousarray(inbound, dtype=np.uint32)
         out = np.zeros(max(n, 1), np.uint32); ng = C.c_uint32()
-        self._check(lib().axc_stage_matching(self._h, n, cnc, _ptr(pairs, C.c_uint32), _ptr(pairs, C.c_uint32),
+        self._check(lib().axc_stage_matching(self._h, n, cnc, _ptr(pairs, C.c_uint32), _ptr(scores, C.c_uint32),
                                              _ptr(ns, C.c_uint32), _ptr(nin, C.c_uint32), omega, delta,
                                              _ptr(out, C.c_uint32), C.byref(ng)), "axc_stage_matching")
         return out[:n], ng.value

@@ -39,7 +39,8 @@ __global__ void k_rate_work(u32 n, const u64 *__restrict__ toff, const u32 *__re
 
 __global__ void k_rate_tier(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u < n) flag[u] = (work[u] > lo && work[u] <= hi) ? 1u : 0u;
+    // the first tier (lo == 0) also takes nodes without incident hyperedges
+    if (u < n) flag[u] = ((lo == 0 || work[u] > lo) && work[u] <= hi) ? 1u : 0u;
 }
 
 struct RateArgs {
@@ -278,60 +279,117 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
 }
 
 // ---------------------------------------------------------------- matching
-// Rounds of mutual proposals (see or_matching in the oracle for the rule). One cooperative launch
-// runs every round with grid-wide barriers; without cooperative launch each phase is a kernel.
-__device__ __forceinline__ void match_propose(u32 n, u32 cnc, const u32 *pairs, const u32 *mate, u32 *ptr,
-                                              u32 *prop, u64 i0, u64 stride) {
-    for (u64 v = i0; v < n; v += stride) {
-        if (mate[v] != NONE) { prop[v] = NONE; continue; }
-        u32 p = ptr[v];
-        while (p < cnc) {
-            u32 w = pairs[v * cnc + p];
-            if (w == NONE) { p = cnc; break; }
-            if (mate[w] == NONE) break;
+// Rounds of proposals (the rule of or_matching in the oracle): A. every unmatched node proposes to
+// its best still-unmatched candidate; B. every node keeps its best proposer by (score, id) with a
+// 64-bit atomicMax (order-independent); C. u and its target v match when v accepted u and v's own
+// proposal was refused, or when both accepted each other. Phase C reads only phase A/B state, so
+// every node is matched at most once per round and the result is deterministic. One cooperative
+// launch runs every round with grid-wide barriers; without cooperative launch each phase is a
+// kernel.
+struct MatchArgs {
+    u32 n, cnc;
+    const u32 *pairs, *scores;
+    u32 *mate, *ptr, *prop;
+    unsigned long long *best;
+    u32 *changed;
+};
+__device__ __forceinline__ void match_propose(const MatchArgs &A, u64 i0, u64 stride) {
+    for (u64 v = i0; v < A.n; v += stride) {
+        A.best[v] = 0;
+        if (A.mate[v] != NONE) { A.prop[v] = NONE; continue; }
+        u32 p = A.ptr[v];
+        while (p < A.cnc) {
+            u32 w = A.pairs[v * A.cnc + p];
+            if (w == NONE) { p = A.cnc; break; }
+            if (A.mate[w] == NONE) break;
             ++p;
         }
-        ptr[v] = p;
-        prop[v] = p < cnc ? pairs[v * cnc + p] : NONE;
+        A.ptr[v] = p;
+        A.prop[v] = p < A.cnc ? A.pairs[v * A.cnc + p] : NONE;
     }
 }
-__device__ __forceinline__ void match_accept(u32 n, const u32 *prop, u32 *mate, u32 *changed, u64 i0,
-                                             u64 stride) {
-    for (u64 v = i0; v < n; v += stride) {
-        u32 w = prop[v];
-        if (w != NONE && w > v && prop[w] == v) {
-            mate[v] = w;
-            mate[w] = (u32)v;
+__device__ __forceinline__ void match_bid(const MatchArgs &A, u64 i0, u64 stride) {
+    for (u64 u = i0; u < A.n; u += stride) {
+        const u32 v = A.prop[u];
+        if (v == NONE) continue;
+        const unsigned long long key = ((unsigned long long)A.scores[u * A.cnc + A.ptr[u]] << 32) | u;
+        atomicMax(&A.best[v], key);
+    }
+}
+__device__ __forceinline__ bool match_acc(const MatchArgs &A, u32 u) {
+    const u32 v = A.prop[u];
+    if (v == NONE) return false;
+    const unsigned long long b = A.best[v];
+    return b != 0 && (u32)b == u;
+}
+__device__ __forceinline__ void match_accept(const MatchArgs &A, u32 *changed, u64 i0, u64 stride) {
+    for (u64 u = i0; u < A.n; u += stride) {
+        if (!match_acc(A, (u32)u)) continue;
+        const u32 v = A.prop[u];
+        if (!match_acc(A, v) || (A.prop[v] == u && u < v)) {
+            A.mate[u] = v;
+            A.mate[v] = (u32)u;
             *changed = 1;
         }
     }
 }
 
-__global__ void k_match_coop(u32 n, u32 cnc, const u32 *__restrict__ pairs, u32 *mate, u32 *ptr, u32 *prop,
-                             u32 rounds, u32 *changed) {
+__global__ void k_match_coop(MatchArgs A, u32 rounds) {
     cg::grid_group grid = cg::this_grid();
     const u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, stride = (u64)gridDim.x * blockDim.x;
     for (u32 r = 0; r < rounds; ++r) {
-        match_propose(n, cnc, pairs, mate, ptr, prop, i0, stride);
+        match_propose(A, i0, stride);
         grid.sync();
-        match_accept(n, prop, mate, &changed[r], i0, stride);
+        match_bid(A, i0, stride);
         grid.sync();
-        if (((volatile u32 *)changed)[r] == 0) break;
+        match_accept(A, &A.changed[r], i0, stride);
+        grid.sync();
+        if (((volatile u32 *)A.changed)[r] == 0) break;
     }
 }
-__global__ void k_match_propose(u32 n, u32 cnc, const u32 *pairs, const u32 *mate, u32 *ptr, u32 *prop,
-                                const u32 *changed, u32 r) {
-    if (r > 0 && changed[r - 1] == 0) return;
-    match_propose(n, cnc, pairs, mate, ptr, prop, (u64)blockIdx.x * blockDim.x + threadIdx.x,
-                  (u64)gridDim.x * blockDim.x);
+__global__ void k_match_phase(MatchArgs A, u32 r, int phase) {
+    if (r > 0 && A.changed[r - 1] == 0) return;  // a previous round reached the fixed point
+    const u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, stride = (u64)gridDim.x * blockDim.x;
+    if (phase == 0) match_propose(A, i0, stride);
+    else if (phase == 1) match_bid(A, i0, stride);
+    else match_accept(A, &A.changed[r], i0, stride);
 }
-__global__ void k_match_accept(u32 n, const u32 *prop, u32 *mate, u32 *changed, u32 r) {
-    if (r > 0 && changed[r - 1] == 0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) changed[r] = 0;
-        return;
-    }
-    match_accept(n, prop, mate, &changed[r], (u64)blockIdx.x * blockDim.x + threadIdx.x,
-                 (u64)gridDim.x * blockDim.x);
+
+// Two-hop pass (see or_matching): unmatched nodes with candidates, sorted by (best candidate, id),
+// pair at even/odd positions of each bucket when the size and inbound-count sums fit.
+__global__ void k_hop_flags(u32 n, u32 cnc, const u32 *__restrict__ pairs, const u32 *__restrict__ mate,
+                            u32 *__restrict__ flag) {
+    u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) flag[v] = (mate[v] == NONE && pairs[(u64)v * cnc] != NONE) ? 1u : 0u;
+}
+__global__ void k_hop_keys(const u32 *__restrict__ ids, const u32 *__restrict__ dm, u32 cnc,
+                           const u32 *__restrict__ pairs, u32 *__restrict__ key) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < *dm) key[i] = pairs[(u64)ids[i] * cnc];
+}
+__global__ void k_hop_heads(const u32 *__restrict__ key, const u32 *__restrict__ dm, u32 nmax, u32 *__restrict__ head) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nmax) return;
+    head[i] = (i < *dm && (i == 0 || key[i] != key[i - 1])) ? 1u : 0u;
+}
+__global__ void k_hop_start(const u32 *__restrict__ head, const u32 *__restrict__ sid, const u32 *__restrict__ dm,
+                            u32 *__restrict__ start) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < *dm && head[i]) start[sid[i]] = i;
+}
+// sid is the exclusive scan of the head flags: the segment of element i is sid[i] + head[i] - 1
+__global__ void k_hop_pair(const u32 *__restrict__ ids, const u32 *__restrict__ key, const u32 *__restrict__ head,
+                           const u32 *__restrict__ sid, const u32 *__restrict__ start, const u32 *__restrict__ dm,
+                           const u32 *__restrict__ nsize, const u32 *__restrict__ nin, u32 omega, u32 delta,
+                           u32 *__restrict__ mate) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 m = *dm;
+    if (i + 1 >= m) return;
+    if (((i - start[sid[i] + head[i] - 1]) & 1u) || key[i + 1] != key[i]) return;
+    const u32 x = ids[i], y = ids[i + 1];
+    if ((u64)nsize[x] + nsize[y] > omega || (u64)nin[x] + nin[y] > delta) return;
+    mate[x] = y;
+    mate[y] = x;
 }
 
 __global__ void k_orphan_flags(u32 n, u32 cnc, const u32 *__restrict__ pairs, u32 *__restrict__ flag) {
@@ -420,6 +478,7 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
                c.d_status};
     u64 *work = c.arena.alloc<u64>(n);
     u32 *flag = c.arena.alloc<u32>(n), *list = c.arena.alloc<u32>(n);
+    fill_u32(c, pairs, NONE, (u64)n * cnc);
     LAUNCH(c, k_rate_work, cdiv((u64)n * 32, 256), 256, 0, n, L.toff, L.touch, L.off, work);
     if (pin_visits) *pin_visits = reduce_sum_u64(c, work, n);
     // tier: one warp per node, table in static smem
@@ -453,15 +512,17 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     c.arena.release(m);
 }
 
-u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u32 *nin, u32 omega, u32 delta,
-             u32 rounds, u32 *groups) {
+u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *scores, const u32 *nsize, const u32 *nin,
+             u32 omega, u32 delta, u32 rounds, u32 *groups) {
     if (n == 0) return 0;
     size_t m = c.arena.mark();
     u32 *mate = c.arena.alloc<u32>(n), *ptr = c.arena.alloc<u32>(n), *prop = c.arena.alloc<u32>(n);
+    unsigned long long *best = c.arena.alloc<unsigned long long>(n);
     u32 *changed = c.arena.alloc<u32>(rounds + 1);
     fill_u32(c, mate, NONE, n);
     AXC_CUDA(cudaMemsetAsync(ptr, 0, (size_t)n * 4, c.stream));
     AXC_CUDA(cudaMemsetAsync(changed, 0, (size_t)(rounds + 1) * 4, c.stream));
+    MatchArgs A{n, cnc, pairs, scores, mate, ptr, prop, best, changed};
     bool done = false;
     if (c.coop_supported) {
         int per_sm = 0;
@@ -470,8 +531,7 @@ u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u
         u32 need = cdiv(n, 256);
         if (grid > need) grid = need;
         if (grid >= 1 && per_sm > 0) {
-            void *args[] = {(void *)&n, (void *)&cnc, (void *)&pairs, (void *)&mate, (void *)&ptr,
-                            (void *)&prop, (void *)&rounds, (void *)&changed};
+            void *args[] = {(void *)&A, (void *)&rounds};
             AXC_CUDA(cudaLaunchCooperativeKernel((void *)k_match_coop, grid, 256, args, 0, c.stream));
             c.launches++;
             done = true;
@@ -479,10 +539,24 @@ u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u
     }
     if (!done) {
         u32 grid = cdiv(n, 256);
-        for (u32 r = 0; r < rounds; ++r) {
-            LAUNCH(c, k_match_propose, grid, 256, 0, n, cnc, pairs, mate, ptr, prop, changed, r);
-            LAUNCH(c, k_match_accept, grid, 256, 0, n, prop, mate, changed, r);
-        }
+        for (u32 r = 0; r < rounds; ++r)
+            for (int ph = 0; ph < 3; ++ph) LAUNCH(c, k_match_phase, grid, 256, 0, A, r, ph);
+    }
+    // two-hop pass
+    {
+        size_t m2 = c.arena.mark();
+        u32 *flag = c.arena.alloc<u32>(n), *ids = c.arena.alloc<u32>(n), *key = c.arena.alloc<u32>(n);
+        u32 *head = c.arena.alloc<u32>(n), *sid = c.arena.alloc<u32>(n), *start = c.arena.alloc<u32>(n);
+        u32 *dm = c.arena.alloc<u32>(1);
+        LAUNCH(c, k_hop_flags, cdiv(n, 256), 256, 0, n, cnc, pairs, mate, flag);
+        compact_indices_dn(c, flag, ids, n, dm);
+        LAUNCH(c, k_hop_keys, cdiv(n, 256), 256, 0, ids, dm, cnc, pairs, key);
+        radix_sort_pairs_dn(c, key, ids, dm, n, bits_for(n - 1));
+        LAUNCH(c, k_hop_heads, cdiv(n, 256), 256, 0, key, dm, n, head);
+        scan_excl_u32(c, head, sid, n);
+        LAUNCH(c, k_hop_start, cdiv(n, 256), 256, 0, head, sid, dm, start);
+        LAUNCH(c, k_hop_pair, cdiv(n, 256), 256, 0, ids, key, head, sid, start, dm, nsize, nin, omega, delta, mate);
+        c.arena.release(m2);
     }
     // orphans
     u32 *flag = c.arena.alloc<u32>(n), *orph = c.arena.alloc<u32>(n);

@@ -71,15 +71,43 @@ struct Ctx {
     u32 launches = 0;
     std::string last_error;
     int coop_supported = 0;
+    // Kernel timer: while on, every launch of the kernel named `prof_name` is bracketed by a pair
+    // of events on the context stream; kernels with a byte model add their algorithmic bytes to
+    // prof_dbytes (device) or prof_hbytes (host).
+    bool prof_on = false;
+    std::string prof_name;
+    std::vector<cudaEvent_t> prof_ev;
+    size_t prof_used = 0;
+    u64 *prof_dbytes = nullptr;
+    u64 prof_hbytes = 0;
+    bool profiling(const char *name) const { return prof_on && prof_name == name; }
+    u64 *prof_counter(const char *name) const { return profiling(name) ? prof_dbytes : nullptr; }
+    cudaEvent_t prof_event() {
+        if (prof_used == prof_ev.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            prof_ev.push_back(e);
+        }
+        return prof_ev[prof_used++];
+    }
 };
 
-// Launch bookkeeping: every kernel launch goes through here so stats can report the count.
+// Launch bookkeeping: every kernel launch goes through here so stats can report the count and
+// the kernel timer can bracket the launches it follows.
 #define LAUNCH(ctx, kern, grid, block, smem, ...)                                              \
     do {                                                                                       \
         if ((grid) > 0) {                                                                      \
+            const bool _prof = (ctx).profiling(#kern);                                         \
+            cudaEvent_t _e0 = _prof ? (ctx).prof_event() : nullptr;                           \
+            if (_e0) cudaEventRecord(_e0, (ctx).stream);                                       \
             kern<<<(grid), (block), (smem), (ctx).stream>>>(__VA_ARGS__);                      \
             (ctx).launches++;                                                                  \
             AXC_CUDA(cudaGetLastError());                                                      \
+            if (_e0) {                                                                         \
+                cudaEvent_t _e1 = (ctx).prof_event();                                          \
+                if (_e1) cudaEventRecord(_e1, (ctx).stream);                                   \
+                else (ctx).prof_used--;                                                        \
+            }                                                                                  \
         }                                                                                      \
     } while (0)
 
@@ -191,6 +219,10 @@ void offsets_from_counts(Ctx &c, const u32 *counts, u64 *out, u64 n);
 // Stable LSD radix sort of (key, value) pairs by the low `bits` bits of key. In place: on
 // return keys/vals hold the sorted data. tmp buffers are taken from the arena.
 void radix_sort_pairs(Ctx &c, u32 *keys, u32 *vals, u64 n, u32 bits);
+// Same with the element count in device memory (*d_n <= n); buffers hold n entries.
+void radix_sort_pairs_dn(Ctx &c, u32 *keys, u32 *vals, const u32 *d_n, u64 n, u32 bits);
+// Stable compaction with the count left in device memory (no host round trip).
+void compact_indices_dn(Ctx &c, const u32 *flags, u32 *out, u64 n, u32 *d_count);
 // Stable sort by a 64-bit key given as (hi, lo) arrays: sorts by lo then by hi.
 void radix_sort_pairs64(Ctx &c, u32 *key_hi, u32 *key_lo, u32 *vals, u64 n, u32 bits_hi, u32 bits_lo);
 // Fill helpers

@@ -130,7 +130,7 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
         u64 visits = 0;
         rating(c, cur, wfx, R.kway ? R.omega_c : R.omega, R.delta, R.cnc, pairs, scores, st ? &visits : nullptr);
         if (st) st->rating_pin_visits += visits;
-        u32 ng = matching(c, cur.n, R.cnc, pairs, cur.nsize, cur.nin, R.kway ? R.omega_c : R.omega, R.delta, 32,
+        u32 ng = matching(c, cur.n, R.cnc, pairs, scores, cur.nsize, cur.nin, R.kway ? R.omega_c : R.omega, R.delta, 32,
                           cur.groups);
         c.arena.release(tmp);
         const float ratio = (float)ng / (float)cur.n;
@@ -553,8 +553,8 @@ int axc_stage_rating(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *node_siz
 int axc_stage_matching(axc_ctx *ctx, uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *scores,
                        const uint32_t *node_size, const uint32_t *inbound, uint32_t omega, uint32_t delta,
                        uint32_t *out_groups, uint32_t *out_num_groups) {
-    (void)scores;
-    if (!ctx || !pairs || !node_size || !inbound || !out_groups || !out_num_groups || cnc == 0) return AXC_EINVAL;
+    if (!ctx || !pairs || !scores || !node_size || !inbound || !out_groups || !out_num_groups || cnc == 0)
+        return AXC_EINVAL;
     for (u64 i = 0; i < (u64)n * cnc; ++i)
         if (pairs[i] != NONE && pairs[i] >= n) return AXC_EINVAL;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -562,13 +562,15 @@ int axc_stage_matching(axc_ctx *ctx, uint32_t n, uint32_t cnc, const uint32_t *p
     try {
         const size_t m = c.arena.mark();
         u32 *dp = c.arena.alloc<u32>((u64)n * cnc + 1), *ds = c.arena.alloc<u32>(n + 1), *di = c.arena.alloc<u32>(n + 1);
+        u32 *dsc = c.arena.alloc<u32>((u64)n * cnc + 1);
         u32 *dg = c.arena.alloc<u32>(n + 1);
         if (n) {
             AXC_CUDA(cudaMemcpyAsync(dp, pairs, (size_t)n * cnc * 4, cudaMemcpyHostToDevice, c.stream));
+            AXC_CUDA(cudaMemcpyAsync(dsc, scores, (size_t)n * cnc * 4, cudaMemcpyHostToDevice, c.stream));
             AXC_CUDA(cudaMemcpyAsync(ds, node_size, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
             AXC_CUDA(cudaMemcpyAsync(di, inbound, (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
         }
-        u32 ng = matching(c, n, cnc, dp, ds, di, omega, delta, 32, dg);
+        u32 ng = matching(c, n, cnc, dp, dsc, ds, di, omega, delta, 32, dg);
         if (n) AXC_CUDA(cudaMemcpyAsync(out_groups, dg, (size_t)n * 4, cudaMemcpyDeviceToHost, c.stream));
         AXC_CUDA(cudaStreamSynchronize(c.stream));
         *out_num_groups = ng;

@@ -36,7 +36,7 @@ void check_input(Ctx &c, u32 n, u32 e, const u64 *off, const u32 *pins, const u3
 void setup_coarsen_kernels(Ctx &c);
 void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 cnc, u32 *pairs,
             u32 *scores, u64 *pin_visits);
-u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u32 *nin, u32 omega,
+u32 matching(Ctx &c, u32 n, u32 cnc, const u32 *pairs, const u32 *scores, const u32 *nsize, const u32 *nin, u32 omega,
              u32 delta, u32 rounds, u32 *groups);
 // greedy packing of the groups of level L (sources/postprocess.cu:16-245); rewrites groups and
 // returns the new group count

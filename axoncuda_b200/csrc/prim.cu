@@ -116,10 +116,11 @@ constexpr int RS_ITEMS = 8;  // rounds of 32 per warp
 constexpr int RS_TILE = RS_WARPS * 32 * RS_ITEMS;
 
 __global__ void k_rs_hist(const u32 *__restrict__ keys, u64 n, u32 shift, u32 *__restrict__ hist,
-                          u32 tiles) {
+                          u32 tiles, const u32 *__restrict__ d_n) {
     __shared__ u32 cnt[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
+    if (d_n) n = *d_n;  // element count resident on the device (tiles past it count nothing)
     const u64 base = (u64)blockIdx.x * RS_TILE;
     for (int j = threadIdx.x; j < RS_TILE; j += blockDim.x) {
         u64 i = base + j;
@@ -131,9 +132,10 @@ __global__ void k_rs_hist(const u32 *__restrict__ keys, u64 n, u32 shift, u32 *_
 
 __global__ void k_rs_scatter(const u32 *__restrict__ kin, const u32 *__restrict__ vin, u32 *__restrict__ kout,
                              u32 *__restrict__ vout, u64 n, u32 shift, const u32 *__restrict__ offs,
-                             u32 tiles) {
+                             u32 tiles, const u32 *__restrict__ d_n) {
     __shared__ u32 wcnt[RS_WARPS][256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (d_n) n = *d_n;
     for (int i = threadIdx.x; i < RS_WARPS * 256; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     __syncthreads();
     const u64 base = (u64)blockIdx.x * RS_TILE + (u64)w * 32 * RS_ITEMS;
@@ -284,6 +286,20 @@ u64 reduce_max_u64(Ctx &c, const u64 *p, u64 n) {
     return r;
 }
 
+void compact_indices_dn(Ctx &c, const u32 *flags, u32 *out, u64 n, u32 *d_count) {
+    if (n == 0) {
+        AXC_CUDA(cudaMemsetAsync(d_count, 0, 4, c.stream));
+        return;
+    }
+    size_t m = c.arena.mark();
+    u32 *f01 = c.arena.alloc<u32>(n);
+    u32 *pos = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_flag_to_u32, grid_for(c, n), 256, 0, flags, f01, n);
+    scan_excl_u32(c, f01, pos, n);
+    LAUNCH(c, k_compact_write, grid_for(c, n), 256, 0, flags, pos, out, n, d_count);
+    c.arena.release(m);
+}
+
 u32 compact_indices(Ctx &c, const u32 *flags, u32 *out, u64 n) {
     if (n == 0) return 0;
     size_t m = c.arena.mark();
@@ -299,16 +315,21 @@ u32 compact_indices(Ctx &c, const u32 *flags, u32 *out, u64 n) {
 }
 
 void radix_sort_pairs(Ctx &c, u32 *keys, u32 *vals, u64 n, u32 bits) {
-    if (n <= 1 || bits == 0) return;
+    radix_sort_pairs_dn(c, keys, vals, nullptr, n, bits);
+}
+
+// Same, with the element count read from device memory (d_n, at most n); no host round trip.
+void radix_sort_pairs_dn(Ctx &c, u32 *keys, u32 *vals, const u32 *d_n, u64 n, u32 bits) {
+    if ((!d_n && n <= 1) || n == 0 || bits == 0) return;
     size_t m = c.arena.mark();
     const u32 tiles = cdiv(n, RS_TILE);
     u32 *k2 = c.arena.alloc<u32>(n), *v2 = c.arena.alloc<u32>(n);
     u32 *hist = c.arena.alloc<u32>((u64)tiles * 256);
     u32 *ka = keys, *va = vals, *kb = k2, *vb = v2;
     for (u32 shift = 0; shift < bits; shift += 8) {
-        LAUNCH(c, k_rs_hist, tiles, 256, 0, ka, n, shift, hist, tiles);
+        LAUNCH(c, k_rs_hist, tiles, 256, 0, ka, n, shift, hist, tiles, d_n);
         scan_excl_u32(c, hist, hist, (u64)tiles * 256);
-        LAUNCH(c, k_rs_scatter, tiles, RS_WARPS * 32, 0, ka, va, kb, vb, n, shift, hist, tiles);
+        LAUNCH(c, k_rs_scatter, tiles, RS_WARPS * 32, 0, ka, va, kb, vb, n, shift, hist, tiles, d_n);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

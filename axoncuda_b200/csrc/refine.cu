@@ -13,6 +13,10 @@
 //  5. prefix sums of cascaded gains; size-excess and inbound-validity of every prefix from sorted
 //     event streams (sources/refinement.cu:239-491); best prefix by best_move_functor
 //     (headers/data_types.cuh:113-136); apply when valid with non-negative prefix gain.
+//
+// Work lists that depend only on the level (hyperedge-length tiers, per-node gain-work bounds)
+// are built once per level. Inside a round every count stays in device memory; the host reads a
+// single word per round (whether moves were applied), which drives the round schedule.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -179,19 +183,36 @@ __device__ __forceinline__ i64 leave_gain(int encourage, u32 w, u32 c) {
     return c == 1 ? (i64)w : 0;
 }
 
-__global__ void k_gain_work(u32 n, const u64 *__restrict__ toff, const u32 *__restrict__ touch,
-                            const u32 *__restrict__ lam, u64 *__restrict__ work) {
+// Per-level bounds of a node's gain work: the partitions adjacent to it in any round number at
+// most min(sum over incident hyperedges of min(|e|, K), K), which sizes its accumulator table; the
+// sum of incident weights bounds its gain.
+__global__ void k_gain_bounds(u32 n, u32 K, const u64 *__restrict__ toff, const u32 *__restrict__ touch,
+                              const u64 *__restrict__ off, const u32 *__restrict__ wfx, u64 *__restrict__ work,
+                              unsigned long long *__restrict__ wmax) {
     const u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (u >= n) return;
-    u64 s = 0;
-    for (u64 j = toff[u] + lane; j < toff[u + 1]; j += 32) s += lam[touch[j]];
+    u64 s = 0, ws = 0;
+    for (u64 j = toff[u] + lane; j < toff[u + 1]; j += 32) {
+        u32 h = touch[j];
+        u64 len = off[h + 1] - off[h];
+        s += len < K ? len : K;
+        ws += wfx[h];
+    }
     s = warp_sum(s);
-    if (lane == 0) work[u] = s;
+    ws = warp_sum(ws);
+    if (lane == 0) {
+        work[u] = s < K ? s : K;
+        atomicMax(wmax, (unsigned long long)ws);
+    }
+}
+__device__ __forceinline__ u32 table_cap(u64 work, u32 cap_max) {
+    u32 cap = 32;
+    while (cap < 2 * work && cap < cap_max) cap <<= 1;
+    return cap;
 }
 
-// Accumulate node u's adjacency to other partitions into (keys, conn, dconn); returns the saving
-// and the total incident weight through the reference arguments (valid in thread t == 0 after
-// the caller's reduction). Threads [0, nt) of the group cooperate hyperedge by hyperedge.
+// Accumulate node u's adjacency to other partitions into (keys, conn, dconn); saving and the
+// total incident weight are summed by the caller over threads [0, nt).
 __device__ __forceinline__ void gain_accumulate(const GainArgs &A, u32 u, u32 p, u32 *keys,
                                                 unsigned long long *conn, u32 *dconn, u32 mask, u32 t, u32 nt,
                                                 i64 &saving, i64 &wtot) {
@@ -252,8 +273,10 @@ __device__ __forceinline__ Cand warp_best(Cand c) {
 constexpr u32 GN_WARP_W = 128;
 constexpr u32 GN_WARPS = 4;
 constexpr u32 GN_BLOCK = 256;
+constexpr u32 GN_BLOCK_W = 4096;
 
-__global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u32 *__restrict__ list, u32 nl) {
+__global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u32 *__restrict__ list, u32 nl,
+                                                             const u64 *__restrict__ work) {
     __shared__ u32 tk[GN_WARPS][2 * GN_WARP_W], td[GN_WARPS][2 * GN_WARP_W];
     __shared__ unsigned long long tcw[GN_WARPS][2 * GN_WARP_W];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -262,11 +285,56 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u
     const u32 u = list[idx], p = A.part[u];
     u32 *keys = tk[w], *dconn = td[w];
     unsigned long long *conn = tcw[w];
-    const u32 cap = 2 * GN_WARP_W;
+    const u32 cap = table_cap(work[u], 2 * GN_WARP_W);
     for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
     __syncwarp();
     i64 saving = 0, wtot = 0;
-    gain_accumulate(A, u, p, keys, conn, dconn, cap - 1, lane, 32, saving, wtot);
+    // 32 incident hyperedges at a time: their metadata loads in parallel, then their census
+    // entries are flattened across the lanes (owner found by a 5-step search over the prefix)
+    const u64 t0 = A.toff[u];
+    const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
+    for (u32 jb = 0; jb < deg; jb += 32) {
+        const u32 j = jb + lane;
+        const bool has = j < deg;
+        const u32 h = has ? A.touch[t0 + j] : 0;
+        const u32 lm = has ? A.lam[h] : 0;
+        const u32 wh = has ? A.wfx[h] : 0;
+        const u64 ah = has ? A.off[h] : 0;
+        const u32 ib = (has && j < nin_u) ? 1u : 0u;
+        wtot += wh;
+        u32 x = lm;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - lm;
+        const u32 chunk = (deg - jb) < 32 ? (deg - jb) : 32;
+        for (u32 fb = 0; fb < total; fb += 32) {
+            const u32 f = fb + lane;
+            u32 lo = 0, hi = chunk - 1;
+            for (int it = 0; it < 5; ++it) {
+                const u32 mid = (lo + hi + 1) >> 1;
+                const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
+                if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
+            }
+            const u32 eo = __shfl_sync(0xFFFFFFFFu, excl, lo);
+            const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, lo);
+            const u32 wo = __shfl_sync(0xFFFFFFFFu, wh, lo);
+            const u32 io = __shfl_sync(0xFFFFFFFFu, ib, lo);
+            if (f >= total) continue;
+            const u64 k = ao + (f - eo);
+            const u32 q = A.cpart[k];
+            if (q == p) {
+                saving += leave_gain(A.encourage, wo, A.ccnt[k]);
+                continue;
+            }
+            const u32 slot = hash_find_or_insert(keys, cap - 1, q);
+            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            atomicAdd(&conn[slot], (unsigned long long)wo);
+            if (io && A.cdcnt[k] > 0) atomicAdd(&dconn[slot], 1u);
+        }
+    }
     saving = warp_sum(saving);
     wtot = warp_sum(wtot);
     __syncwarp();
@@ -289,7 +357,7 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u
 }
 
 __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A, const u32 *__restrict__ list, u32 nl, u32 cap_max,
-                                                        u32 *gtab) {
+                                                        u32 *gtab, const u64 *__restrict__ work) {
     extern __shared__ unsigned long long dyn64[];
     __shared__ i64 red[2][32];
     __shared__ Cand cred[32];
@@ -297,9 +365,9 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A, const u32 *
         const u32 u = list[idx], p = A.part[u];
         unsigned long long *conn;
         u32 *keys, *dconn;
-        const u32 cap = cap_max;
+        const u32 cap = table_cap(work[u], cap_max);
         if (gtab) {
-            u32 *base = gtab + (u64)blockIdx.x * 4 * cap;
+            u32 *base = gtab + (u64)blockIdx.x * 4 * cap_max;  // this block's slice
             conn = (unsigned long long *)base;
             keys = base + 2 * cap;
             dconn = keys + cap;
@@ -344,30 +412,31 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A, const u32 *
     }
 }
 
+__global__ void k_tier(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
+    u32 u = blockIdx.x * blockDim.x + threadIdx.x;
+    // the first tier (lo == 0) also takes nodes without incident hyperedges
+    if (u < n) flag[u] = ((lo == 0 || work[u] > lo) && work[u] <= hi) ? 1u : 0u;
+}
+
 // ------------------------------------------------------------------ ranking
 __global__ void k_move_flags(u32 n, const u32 *__restrict__ target, u32 *__restrict__ flag) {
     u32 v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) flag[v] = target[v] != NONE ? 1u : 0u;
 }
-__global__ void k_move_keys(const u32 *__restrict__ mv, u32 M, const i64 *__restrict__ gain, u64 gmax,
-                            u32 *__restrict__ hi, u32 *__restrict__ lo) {
+__global__ void k_move_keys(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const i64 *__restrict__ gain,
+                            u64 gbound, u32 *__restrict__ hi, u32 *__restrict__ lo) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
-    u64 k = gmax - (u64)gain[mv[i]];  // ascending key = descending gain
+    if (i >= *dM) return;
+    u64 k = gbound - (u64)gain[mv[i]];  // ascending key = descending gain
     hi[i] = (u32)(k >> 32);
     lo[i] = (u32)k;
 }
-__global__ void k_gain_max(const u32 *__restrict__ mv, u32 M, const i64 *__restrict__ gain,
-                           unsigned long long *__restrict__ out) {
+__global__ void k_set_rank(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 *__restrict__ rank) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    u64 g = i < M ? (u64)gain[mv[i]] : 0;
-    g = warp_max_u64(g);
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)g);
+    if (i < *dM) rank[mv[i]] = i;
 }
-__global__ void k_set_rank(const u32 *__restrict__ mv, u32 M, u32 *__restrict__ rank) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M) rank[mv[i]] = i;
-}
+// small per-round counters derived on the device: [0] M, [1] 2M, [2] inbound events, [3] T
+__global__ void k_twice(const u32 *__restrict__ dM, u32 *__restrict__ out) { *out = 2 * *dM; }
 
 // ------------------------------------------------------------------ cascade
 constexpr u32 CC_WARPS = 4;
@@ -378,16 +447,36 @@ struct CascadeArgs {
     u32 e;
     int encourage;
     const u64 *off;
-    const u32 *pins, *wfx, *lam, *cpart, *ccnt, *rank, *part, *target;
+    const u32 *pins, *nsrc, *wfx, *lam, *cpart, *ccnt, *cdcnt, *rank, *part, *target;
     unsigned long long *g2;
+    // inbound-set transitions (INCC): a (partition, hyperedge) destination count going 0 -> 1 or
+    // 1 -> 0 at a move's rank; appended as (partition, rank, +-1)
+    int track;
+    u32 *tp, *tr;
+    int32_t *tdv;
+    u32 *dT;
+    u64 tcap;
     u32 *status;
 };
 
-// Sweep the movers (sorted by rank) of one hyperedge sequentially.
-__device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, u32 m, u32 *tk, u32 *tc, u32 mask) {
+constexpr u32 MV_DST = 0x80000000u;  // mover flag in the node field: the pin is a destination
+
+__device__ __forceinline__ void emit_transition(const CascadeArgs &A, u32 p, u32 r, int32_t d) {
+    const u32 s = atomicAdd(A.dT, 1u);
+    if (s >= A.tcap) { atomicExch(A.status, DEV_BAD_INDEX); return; }
+    A.tp[s] = p;
+    A.tr[s] = r;
+    A.tdv[s] = d;
+}
+
+// Sweep the movers of one hyperedge sequentially in rank order. mv[i] = rank << 32 | dst flag |
+// node; tc / td hold the hyperedge's pins / destination pins per partition (hash slots in tk).
+__device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, u32 m, u32 *tk, u32 *tc, u32 *td,
+                              u32 mask) {
     const u32 w = A.wfx[h];
     for (u32 i = 0; i < m; ++i) {
-        const u32 v = (u32)mv[i];
+        const u32 lowv = (u32)mv[i], r = (u32)(mv[i] >> 32);
+        const u32 v = lowv & ~MV_DST;
         const u32 p = A.part[v], q = A.target[v];
         const u32 sp = hash_find_or_insert(tk, mask, p), sq = hash_find_or_insert(tk, mask, q);
         if (sp == NONE || sq == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
@@ -396,17 +485,23 @@ __device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, u32 m,
         atomicAdd(&A.g2[v], (unsigned long long)d);
         tc[sp] = cp - 1;
         tc[sq] = tc[sq] + 1;
+        if (A.track && (lowv & MV_DST)) {
+            if (td[sp] == 1) emit_transition(A, p, r, -1);
+            if (td[sq] == 0) emit_transition(A, q, r, +1);
+            td[sp] -= 1;
+            td[sq] += 1;
+        }
     }
 }
 
-__global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big) {
+__global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__restrict__ nbig) {
     __shared__ u64 mvs[CC_WARPS][CC_MOV];
-    __shared__ u32 tk[CC_WARPS][CC_TAB], tc[CC_WARPS][CC_TAB];
+    __shared__ u32 tk[CC_WARPS][CC_TAB], tc[CC_WARPS][CC_TAB], td[CC_WARPS][CC_TAB];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 h = blockIdx.x * CC_WARPS + w;
     if (h >= A.e) return;
-    const u64 a = A.off[h], b = A.off[h + 1];
-    // collect movers (rank << 32 | node)
+    const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
+    // collect movers (rank << 32 | dst flag | node)
     u32 m = 0;
     for (u64 base = a; base < b; base += 32) {
         u64 k = base + lane;
@@ -415,14 +510,14 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big) {
         u32 bal = __ballot_sync(0xFFFFFFFFu, mvr);
         if (mvr) {
             u32 pos = m + __popc(bal & ((1u << lane) - 1u));
-            if (pos < CC_MOV) mvs[w][pos] = ((u64)r << 32) | v;
+            if (pos < CC_MOV) mvs[w][pos] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
         }
         m += __popc(bal);
     }
     if (m == 0) return;
     const u32 lm = A.lam[h];
     if (m > CC_MOV || 2 * (lm + 2 * m) > CC_TAB) {
-        if (lane == 0) big[h] = 1;
+        if (lane == 0) big[atomicAdd(nbig, 1u)] = h;  // handled by the block kernel
         return;
     }
     __syncwarp();
@@ -441,90 +536,82 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big) {
     // table of partition counts from the census
     u32 cap = 32;
     while (cap < 2 * (lm + 2 * m)) cap <<= 1;
-    for (u32 i = lane; i < cap; i += 32) { tk[w][i] = NONE; tc[w][i] = 0; }
+    for (u32 i = lane; i < cap; i += 32) { tk[w][i] = NONE; tc[w][i] = 0; td[w][i] = 0; }
     __syncwarp();
     for (u32 i = lane; i < lm; i += 32) {
         u32 s = hash_find_or_insert(tk[w], cap - 1, A.cpart[a + i]);
-        if (s != NONE) tc[w][s] = A.ccnt[a + i];
+        if (s != NONE) { tc[w][s] = A.ccnt[a + i]; td[w][s] = A.cdcnt[a + i]; }
     }
     __syncwarp();
-    if (lane == 0) cascade_sweep(A, h, mvs[w], m, tk[w], tc[w], cap - 1);
+    if (lane == 0) cascade_sweep(A, h, mvs[w], m, tk[w], tc[w], td[w], cap - 1);
 }
 
-// Large hyperedges: one block each, movers and tables in global scratch.
-__global__ void k_cascade_big(CascadeArgs A, const u32 *__restrict__ list, u32 nl, u64 *scratch_mv, u32 *scratch_tab,
-                              const u64 *__restrict__ mv_off, const u64 *__restrict__ tab_off) {
-    if (blockIdx.x >= nl) return;
-    const u32 h = list[blockIdx.x];
-    const u64 a = A.off[h], b = A.off[h + 1];
-    u64 *mvs = scratch_mv + mv_off[blockIdx.x];
-    const u32 lm = A.lam[h];
+// Hyperedges with many movers: one block at a time per hyperedge, movers and table in this
+// block's slice of a scratch region sized by the level's largest hyperedge.
+__global__ void k_cascade_big(CascadeArgs A, const u32 *__restrict__ list, const u32 *__restrict__ nl, u64 *scratch_mv,
+                              u32 *scratch_tab, u64 mv_cap, u64 tab_cap) {
     __shared__ u32 cntm;
-    if (threadIdx.x == 0) cntm = 0;
-    __syncthreads();
-    for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
-        u32 v = A.pins[k], r = A.rank[v];
-        if (r != NONE) mvs[atomicAdd(&cntm, 1u)] = ((u64)r << 32) | v;
-    }
-    __syncthreads();
-    const u32 m = cntm;
-    // sort by rank: odd-even transposition over the block (m is bounded by the hyperedge size)
-    for (u32 phase = 0; phase < m; ++phase) {
-        for (u32 i = 2 * threadIdx.x + (phase & 1); i + 1 < m; i += 2 * blockDim.x) {
-            u64 x = mvs[i], y = mvs[i + 1];
-            if (x > y) { mvs[i] = y; mvs[i + 1] = x; }
+    u64 *mvs = scratch_mv + (u64)blockIdx.x * mv_cap;
+    for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
+        const u32 h = list[idx];
+        const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
+        const u32 lm = A.lam[h];
+        if (threadIdx.x == 0) cntm = 0;
+        __syncthreads();
+        for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
+            u32 v = A.pins[k], r = A.rank[v];
+            if (r != NONE) mvs[atomicAdd(&cntm, 1u)] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
         }
         __syncthreads();
+        const u32 m = cntm;
+        // sort by rank: odd-even transposition (m is bounded by the hyperedge size)
+        for (u32 phase = 0; phase < m; ++phase) {
+            for (u32 i = 2 * threadIdx.x + (phase & 1); i + 1 < m; i += 2 * blockDim.x) {
+                u64 x = mvs[i], y = mvs[i + 1];
+                if (x > y) { mvs[i] = y; mvs[i + 1] = x; }
+            }
+            __syncthreads();
+        }
+        u32 cap = 32;
+        while (cap < 2 * (lm + 2 * m)) cap <<= 1;
+        u32 *tk = scratch_tab + (u64)blockIdx.x * tab_cap, *tc = tk + cap, *td = tc + cap;
+        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tk[i] = NONE; tc[i] = 0; td[i] = 0; }
+        __syncthreads();
+        for (u32 i = threadIdx.x; i < lm; i += blockDim.x) {
+            u32 s = hash_find_or_insert(tk, cap - 1, A.cpart[a + i]);
+            if (s != NONE) { tc[s] = A.ccnt[a + i]; td[s] = A.cdcnt[a + i]; }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) cascade_sweep(A, h, mvs, m, tk, tc, td, cap - 1);
+        __syncthreads();
     }
-    u32 cap = 32;
-    while (cap < 2 * (lm + 2 * m)) cap <<= 1;
-    u32 *tk = scratch_tab + tab_off[blockIdx.x], *tc = tk + cap;
-    for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tk[i] = NONE; tc[i] = 0; }
-    __syncthreads();
-    for (u32 i = threadIdx.x; i < lm; i += blockDim.x) {
-        u32 s = hash_find_or_insert(tk, cap - 1, A.cpart[a + i]);
-        if (s != NONE) tc[s] = A.ccnt[a + i];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) cascade_sweep(A, h, mvs, m, tk, tc, cap - 1);
-}
-__global__ void k_big_sizes(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ off, const u32 *__restrict__ lam,
-                            u64 *__restrict__ mvsz, u64 *__restrict__ tabsz) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == nl) { mvsz[i] = 0; tabsz[i] = 0; }
-    if (i >= nl) return;
-    u32 h = list[i];
-    u64 len = off[h + 1] - off[h];
-    u64 cap = 32;
-    while (cap < 2 * (lam[h] + 2 * len)) cap <<= 1;
-    mvsz[i] = len;
-    tabsz[i] = 2 * cap;
 }
 
 // ------------------------------------------------------------------ prefix and validity
-__global__ void k_gather_g2(const u32 *__restrict__ mv, u32 M, const unsigned long long *__restrict__ g2,
-                            i64 *__restrict__ G) {
+__global__ void k_gather_g2(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 nmax,
+                            const unsigned long long *__restrict__ g2, i64 *__restrict__ G) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M) G[i] = (i64)g2[mv[i]];
+    if (i < nmax) G[i] = i < *dM ? (i64)g2[mv[i]] : 0;
 }
-__global__ void k_incl_fix(const i64 *__restrict__ x, i64 *__restrict__ ex, u32 M) {  // ex := ex + x
+__global__ void k_incl_fix(const i64 *__restrict__ x, i64 *__restrict__ ex, u32 nmax) {  // ex := ex + x
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M) ex[i] += x[i];
+    if (i < nmax) ex[i] += x[i];
 }
 
 // size events: 2r = leave p, 2r+1 = join q
-__global__ void k_size_events(const u32 *__restrict__ mv, u32 M, const u32 *__restrict__ part,
+__global__ void k_size_events(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ part,
                               const u32 *__restrict__ target, u32 *__restrict__ key, u32 *__restrict__ val) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 2 * M) return;
+    if (i >= 2 * *dM) return;
     u32 v = mv[i >> 1];
     key[i] = (i & 1) ? target[v] : part[v];
     val[i] = i;
 }
-__global__ void k_size_delta(const u32 *__restrict__ mv, const u32 *__restrict__ val, u32 ne,
-                             const u32 *__restrict__ nsize, i64 *__restrict__ d) {
+__global__ void k_size_delta(const u32 *__restrict__ mv, const u32 *__restrict__ val, const u32 *__restrict__ dne,
+                             u32 nmax, const u32 *__restrict__ nsize, i64 *__restrict__ d) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ne) return;
+    if (i >= nmax) return;
+    if (i >= *dne) { d[i] = 0; return; }
     u32 ev = val[i];
     i64 s = nsize[mv[ev >> 1]];
     d[i] = (ev & 1) ? s : -s;
@@ -538,9 +625,10 @@ __device__ __forceinline__ u32 lower_bound_u32(const u32 *a, u32 len, u32 x) {
     return lo;
 }
 __global__ void k_size_flags(const u32 *__restrict__ key, const u32 *__restrict__ val, const i64 *__restrict__ d,
-                             const i64 *__restrict__ E, u32 ne, const u64 *__restrict__ psize, u64 omega,
-                             unsigned long long *__restrict__ Vs) {
+                             const i64 *__restrict__ E, const u32 *__restrict__ dne, const u64 *__restrict__ psize,
+                             u64 omega, unsigned long long *__restrict__ Vs) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 ne = *dne;
     if (i >= ne) return;
     u32 p = key[i];
     u32 st = lower_bound_u32(key, ne, p);
@@ -551,126 +639,64 @@ __global__ void k_size_flags(const u32 *__restrict__ key, const u32 *__restrict_
     if (exa != exb) atomicAdd(&Vs[val[i] >> 1], (unsigned long long)(exa - exb));
 }
 
-// inbound events: mover r, its i-th inbound hyperedge: 2i = leave p (-1), 2i+1 = join q (+1)
-__global__ void k_inb_counts(const u32 *__restrict__ mv, u32 M, const u32 *__restrict__ nin, u32 *__restrict__ c) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < M) c[i] = 2 * nin[mv[i]];
-}
-__global__ void k_inb_events(const u32 *__restrict__ mv, u32 M, const u64 *__restrict__ base,
-                             const u64 *__restrict__ toff, const u32 *__restrict__ touch, const u32 *__restrict__ nin,
-                             const u32 *__restrict__ part, const u32 *__restrict__ target, u32 *__restrict__ keyH,
-                             u32 *__restrict__ keyP, u32 *__restrict__ val) {
-    const u32 r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (r >= M) return;
-    const u32 v = mv[r];
-    const u64 b0 = base[r], t0 = toff[v];
-    const u32 ni = nin[v], p = part[v], q = target[v];
-    for (u32 i = lane; i < ni; i += 32) {
-        u32 h = touch[t0 + i];
-        u64 e0 = b0 + 2 * i;
-        keyH[e0] = h; keyP[e0] = p; val[e0] = (u32)e0;
-        keyH[e0 + 1] = h; keyP[e0 + 1] = q; val[e0 + 1] = (u32)(e0 + 1);
-    }
-}
-__global__ void k_gather_by(const u32 *__restrict__ src, const u32 *__restrict__ idx, u32 *__restrict__ dst, u64 n) {
+__global__ void k_gather_by_dn(const u32 *__restrict__ src, const u32 *__restrict__ idx, u32 *__restrict__ dst,
+                               const u32 *__restrict__ dn) {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[idx[i]];
+    if (i < *dn) dst[i] = src[idx[i]];
 }
-__device__ __forceinline__ u32 upper_bound_u64d(const u64 *a, u32 len, u64 x) {
-    u32 lo = 0, hi = len;
-    while (lo < hi) {
-        u32 mid = (lo + hi) >> 1;
-        if (a[mid] <= x) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-// per sorted event: hyperedge, partition, sign, rank; heads of (p,h) segments
-__global__ void k_inb_decode(const u32 *__restrict__ val, const u32 *__restrict__ keyP, u64 ne, const u64 *__restrict__ base,
-                             u32 M, const u32 *__restrict__ mv, const u64 *__restrict__ toff,
-                             const u32 *__restrict__ touch, u32 *__restrict__ ev_h, u32 *__restrict__ ev_r,
-                             i64 *__restrict__ ev_d, u32 *__restrict__ head) {
+__global__ void k_seg_heads(const u32 *__restrict__ a, const u32 *__restrict__ b, const u32 *__restrict__ dn, u64 nmax,
+                            u32 *__restrict__ head) {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ne) return;
-    u32 ev = val[i];
-    u32 r = upper_bound_u64d(base, M + 1, ev) - 1;
-    u32 k = (u32)((ev - base[r]) >> 1);
-    ev_h[i] = touch[toff[mv[r]] + k];
-    ev_r[i] = r;
-    ev_d[i] = (ev & 1) ? 1 : -1;
-    (void)keyP;
-}
-__global__ void k_seg_heads(const u32 *__restrict__ a, const u32 *__restrict__ b, u64 ne, u32 *__restrict__ head) {
-    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ne) return;
+    if (i >= nmax) return;
+    if (i >= *dn) { head[i] = 0; return; }
     head[i] = (i == 0 || a[i] != a[i - 1] || (b && b[i] != b[i - 1])) ? 1u : 0u;
 }
-__global__ void k_seg_start(const u32 *__restrict__ head, const u32 *__restrict__ sid, u64 ne, u32 *__restrict__ start) {
+__global__ void k_seg_start(const u32 *__restrict__ head, const u32 *__restrict__ sid, const u32 *__restrict__ dn,
+                            u32 *__restrict__ start) {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < ne && head[i]) start[sid[i]] = (u32)i;
+    if (i < *dn && head[i]) start[sid[i]] = (u32)i;
 }
-__device__ __forceinline__ u32 census_dcnt(const u64 *off, const u32 *lam, const u32 *cpart, const u32 *cdcnt, u32 h,
-                                           u32 p) {
-    const u64 a = off[h];
-    for (u32 j = 0; j < lam[h]; ++j)
-        if (cpart[a + j] == p) return cdcnt[a + j];
-    return 0;
+__global__ void k_clamp_count(u32 *__restrict__ cnt, u64 cap) {
+    if (*cnt > cap) *cnt = (u32)cap;
 }
-// transitions of a (partition, hyperedge) destination count through 0
-__global__ void k_inb_trans(const u32 *__restrict__ keyP, const u32 *__restrict__ ev_h, const u32 *__restrict__ ev_r,
-                            const i64 *__restrict__ ev_d, const i64 *__restrict__ E, const u32 *__restrict__ head,
-                            const u32 *__restrict__ sid, const u32 *__restrict__ start, u64 ne,
-                            const u64 *__restrict__ off, const u32 *__restrict__ lam, const u32 *__restrict__ cpart,
-                            const u32 *__restrict__ cdcnt, u32 *__restrict__ tflag, int32_t *__restrict__ tdelta) {
+// transition keys: (partition, rank) in one word when both fit, else the rank alone (the
+// partition is then a second stable pass)
+__global__ void k_trans_keys(const u32 *__restrict__ dT, u64 nmax, const u32 *__restrict__ tp,
+                             const u32 *__restrict__ tr, u32 rbits, int combined, u32 *__restrict__ key,
+                             u32 *__restrict__ perm) {
+    u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= *dT) return;
+    key[j] = combined ? ((tp[j] << rbits) | tr[j]) : tr[j];
+    perm[j] = (u32)j;
+}
+// after ordering by (p, r): partition, rank and delta of position i
+__global__ void k_trans_perm(const u32 *__restrict__ perm, const u32 *__restrict__ dT, u64 nmax,
+                             const u32 *__restrict__ tp, const u32 *__restrict__ tr, const int32_t *__restrict__ td,
+                             u32 *__restrict__ sp, u32 *__restrict__ sr, i64 *__restrict__ sd) {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ne) return;
-    const u32 st = start[sid[i]];
-    const i64 base = census_dcnt(off, lam, cpart, cdcnt, ev_h[i], keyP[i]);
-    const i64 before = base + (E[i] - E[st]);
-    const i64 after = before + ev_d[i];
-    int32_t t = 0;
-    if (before == 0 && after > 0) t = 1;
-    if (before > 0 && after == 0) t = -1;
-    tflag[i] = t != 0;
-    tdelta[i] = t;
-    (void)head;
-}
-// transition j (in (p, h, r) order): partition, rank, +-1
-__global__ void k_trans_gather(const u32 *__restrict__ idx, u32 T, const u32 *__restrict__ keyP,
-                               const u32 *__restrict__ ev_r, const int32_t *__restrict__ tdelta, u32 *__restrict__ tp,
-                               u32 *__restrict__ tr, int32_t *__restrict__ td) {
-    u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= T) return;
-    tp[j] = keyP[idx[j]];
-    tr[j] = ev_r[idx[j]];
-    td[j] = tdelta[idx[j]];
-}
-// after ordering by (p, r): sorted rank and delta of position i
-__global__ void k_trans_perm(const u32 *__restrict__ perm, u32 T, const u32 *__restrict__ tr,
-                             const int32_t *__restrict__ td, u32 *__restrict__ sr, i64 *__restrict__ sd) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= T) return;
-    sr[i] = tr[perm[i]];
-    sd[i] = td[perm[i]];
+    if (i >= nmax) return;
+    if (i >= *dT) { sd[i] = 0; return; }
+    const u32 j = perm[i];
+    sp[i] = tp[j];
+    sr[i] = tr[j];
+    sd[i] = td[j];
 }
 // per partition, the running inbound-set size along the move sequence; an event that makes the
 // partition exceed delta adds +1 at its rank, one that brings it back adds -1. The first event of a
 // partition assumes it started valid (kernels/refinement.cu:632-651).
 __global__ void k_trans_flags(const u32 *__restrict__ sp, const u32 *__restrict__ sr, const i64 *__restrict__ sd,
-                              const i64 *__restrict__ E, const u32 *__restrict__ sid, const u32 *__restrict__ start,
-                              u32 T, const u64 *__restrict__ pinb, u64 delta, unsigned long long *__restrict__ Vi) {
+                              const i64 *__restrict__ E, const u32 *__restrict__ head, const u32 *__restrict__ sid,
+                              const u32 *__restrict__ start, const u32 *__restrict__ dT, const u64 *__restrict__ pinb,
+                              u64 delta, unsigned long long *__restrict__ Vi) {
     u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= T) return;
+    if (j >= *dT) return;
     const u32 p = sp[j];
-    const u32 st = start[sid[j]];
+    const u32 st = start[sid[j] + head[j] - 1];
     const i64 before = (i64)pinb[p] + (E[j] - E[st]);
     const i64 after = before + sd[j];
     const bool was_bad = (j != st) && before > (i64)delta;
     const bool is_bad = after > (i64)delta;
     if (was_bad != is_bad) atomicAdd(&Vi[sr[j]], (unsigned long long)(i64)(is_bad ? 1 : -1));
-}
-__global__ void k_iota(u32 *p, u32 n) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = i;
 }
 
 // best prefix (best_move_functor): inbound-valid first, then fewer size violations, then larger
@@ -687,10 +713,11 @@ __device__ __forceinline__ bool best_better(const Best &b, const Best &a) {  // 
     if (a.g != b.g) return b.g > a.g;
     return b.r < a.r;
 }
-__global__ void k_best(const i64 *__restrict__ G, const i64 *__restrict__ Vs, const i64 *__restrict__ Vi, u32 M,
-                       Best *__restrict__ out) {
+__global__ void k_best(const i64 *__restrict__ G, const i64 *__restrict__ Vs, const i64 *__restrict__ Vi,
+                       const u32 *__restrict__ dM, Best *__restrict__ out) {
     __shared__ Best sh[256];
     Best b{0, 0, 0, 0xFFFFFFFFu};
+    const u32 M = *dM;
     for (u32 r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
         Best c{Vi ? (Vi[r] == 0 ? 1u : 0u) : 1u, Vs[r], G[r], r};
         if (b.r == 0xFFFFFFFFu || best_better(c, b)) b = c;
@@ -710,7 +737,7 @@ __global__ void k_best_final(const Best *__restrict__ in, u32 nb, const i64 *__r
     for (u32 i = 1; i < nb; ++i)
         if (in[i].r != 0xFFFFFFFFu && (x.r == 0xFFFFFFFFu || best_better(in[i], x))) x = in[i];
     *out = x;
-    const i64 vi = Vi ? Vi[x.r] : 0;
+    const i64 vi = (Vi && x.r != 0xFFFFFFFFu) ? Vi[x.r] : 0;
     *apply = (x.r != 0xFFFFFFFFu && x.vs <= 0 && vi <= 0 && x.g >= 0) ? 1u : 0u;
 }
 __global__ void k_apply(const u32 *__restrict__ mv, const u32 *__restrict__ target, const Best *__restrict__ best,
@@ -719,11 +746,6 @@ __global__ void k_apply(const u32 *__restrict__ mv, const u32 *__restrict__ targ
     if (!*apply || i > best->r) return;
     u32 v = mv[i];
     part[v] = target[v];
-}
-
-__global__ void k_rate_tier_g(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
-    u32 u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u < n) flag[u] = (work[u] > lo && work[u] <= hi) ? 1u : 0u;
 }
 
 GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp, const Census &cs, const u32 *part,
@@ -738,70 +760,127 @@ GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp,
     return A;
 }
 
-void run_gains(Ctx &c, const DLevel &L, const GainArgs &A) {
-    const u32 n = L.n;
-    size_t m = c.arena.mark();
-    u64 *work = c.arena.alloc<u64>(n);
-    u32 *flag = c.arena.alloc<u32>(n), *list = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_gain_work, cdiv((u64)n * 32, 256), 256, 0, n, L.toff, L.touch, A.lam, work);
-    // warp tier: adjacency work <= 128 -> 256-slot table
-    LAUNCH(c, k_rate_tier_g, cdiv(n, 256), 256, 0, n, work, 0ull, (u64)GN_WARP_W, flag);
-    u32 nl = compact_indices(c, flag, list, n);
-    LAUNCH(c, k_gain_warp, cdiv(nl, GN_WARPS), GN_WARPS * 32, 0, A, list, nl);
-    // block tier: <= 4096 -> 8192-slot table in dynamic smem (16 B per slot)
-    LAUNCH(c, k_rate_tier_g, cdiv(n, 256), 256, 0, n, work, (u64)GN_WARP_W, 4096ull, flag);
-    nl = compact_indices(c, flag, list, n);
-    LAUNCH(c, k_gain_block, nl, GN_BLOCK, 8192 * 16, A, list, nl, 8192u, (u32 *)nullptr);
-    // heavy tier: global tables
-    LAUNCH(c, k_rate_tier_g, cdiv(n, 256), 256, 0, n, work, 4096ull, ~0ull, flag);
-    nl = compact_indices(c, flag, list, n);
-    if (nl) {
-        u64 wmax = reduce_max_u64(c, work, n);
-        u32 cap = 64;
-        while (cap < 2 * wmax && cap < (1u << 28)) cap <<= 1;
-        u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
-        u32 *gtab = c.arena.alloc<u32>((u64)grid * 4 * cap);
-        LAUNCH(c, k_gain_block, grid, GN_BLOCK, 0, A, list, nl, cap, gtab);
-    }
-    c.arena.release(m);
-}
-
 }  // namespace
 
+// Work lists of one level for the census (hyperedge length tiers) and the gains (node gain-work
+// bound tiers), plus the bounds that size per-round buffers. Built once per level.
+struct LevelPrep {
+    u32 *hblock = nullptr, n_hblock = 0;       // 256 < |e| <= 4096
+    u32 *hhuge = nullptr, n_hhuge = 0;         // |e| > 4096
+    u64 *huge_tab = nullptr, huge_tot = 0;     // table offsets of the huge hyperedges
+    u32 *ntier[3] = {nullptr, nullptr, nullptr};
+    u32 ncount[3] = {0, 0, 0};
+    u64 *work = nullptr;     // per-node table bound of the gains
+    u64 heavy_work_max = 0;  // largest gain-work bound of the heavy tier
+    u64 gain_bound = 0;      // no gain exceeds this (sum of incident weights)
+    u64 max_len = 0;         // largest hyperedge
+    u64 dst_pins = 0;        // destination pins (bounds the inbound events: 2 per pin)
+};
 
 void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_census_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 2 * CS_BLOCK_CAP * 4));
-    AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 16));
+    AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
 }
 
-Census build_census(Ctx &c, const DLevel &L, const u32 *part) {
+static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
+    LevelPrep lp;
+    const u32 e = L.e, n = L.n;
+    if (e) {
+        u32 *flag = c.arena.alloc<u32>(e);
+        lp.hblock = c.arena.alloc<u32>(e);
+        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
+        lp.n_hblock = compact_indices(c, flag, lp.hblock, e);
+        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
+        lp.hhuge = c.arena.alloc<u32>(e);
+        lp.n_hhuge = compact_indices(c, flag, lp.hhuge, e);
+        if (lp.n_hhuge) {
+            lp.huge_tab = c.arena.alloc<u64>(lp.n_hhuge + 1);
+            LAUNCH(c, k_tab_sizes, cdiv(lp.n_hhuge + 1, 256), 256, 0, lp.hhuge, lp.n_hhuge, L.off, lp.huge_tab);
+            scan_excl_u64(c, lp.huge_tab, lp.huge_tab, lp.n_hhuge + 1);
+            lp.huge_tot = fetch1(c, lp.huge_tab + lp.n_hhuge);
+        }
+    }
+    if (n) {
+        u64 *work = c.arena.alloc<u64>(n);
+        lp.work = work;
+        unsigned long long *wm = c.arena.alloc<unsigned long long>(1);
+        AXC_CUDA(cudaMemsetAsync(wm, 0, 8, c.stream));
+        LAUNCH(c, k_gain_bounds, cdiv((u64)n * 32, 256), 256, 0, n, K, L.toff, L.touch, L.off, wfx, work, wm);
+        u32 *flag = c.arena.alloc<u32>(n);
+        const u64 lim[4] = {0, GN_WARP_W, GN_BLOCK_W, ~0ull};
+        for (int t = 0; t < 3; ++t) {
+            lp.ntier[t] = c.arena.alloc<u32>(n);
+            LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, work, lim[t], lim[t + 1], flag);
+            lp.ncount[t] = compact_indices(c, flag, lp.ntier[t], n);
+        }
+        lp.gain_bound = fetch1(c, (const u64 *)wm);
+        if (lp.ncount[2]) lp.heavy_work_max = reduce_max_u64(c, work, n);
+    }
+    return lp;
+}
+
+static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *part, Census &cs) {
+    cs.beg = L.off;
+    if (L.e == 0) return;
+    CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status};
+    LAUNCH(c, k_census_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A);
+    if (lp.n_hblock)
+        LAUNCH(c, k_census_block, lp.n_hblock, 256, 4 * 2 * CS_BLOCK_CAP * 4, lp.hblock, lp.n_hblock, A,
+               (u32 *)nullptr, (const u64 *)nullptr);
+    if (lp.n_hhuge) {
+        size_t m = c.arena.mark();
+        u32 *gtab = c.arena.alloc<u32>(4 * lp.huge_tot);
+        LAUNCH(c, k_census_block, lp.n_hhuge, 512, 0, lp.hhuge, lp.n_hhuge, A, gtab, (const u64 *)lp.huge_tab);
+        c.arena.release(m);
+    }
+}
+
+static Census alloc_census(Ctx &c, const DLevel &L) {
     Census cs;
-    const u32 e = L.e;
     cs.beg = L.off;
     cs.part = c.arena.alloc<u32>(L.P ? L.P : 1);
     cs.cnt = c.arena.alloc<u32>(L.P ? L.P : 1);
     cs.dcnt = c.arena.alloc<u32>(L.P ? L.P : 1);
-    cs.lam = c.arena.alloc<u32>(e ? e : 1);
-    if (e == 0) return cs;
-    CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status};
-    LAUNCH(c, k_census_warp, cdiv(e, CS_WARPS), CS_WARPS * 32, 0, e, A);
-    size_t m = c.arena.mark();
-    u32 *flag = c.arena.alloc<u32>(e), *list = c.arena.alloc<u32>(e);
-    LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
-    u32 nb = compact_indices(c, flag, list, e);
-    if (nb)
-        LAUNCH(c, k_census_block, nb, 256, 4 * 2 * CS_BLOCK_CAP * 4, list, nb, A, (u32 *)nullptr,
-               (const u64 *)nullptr);
-    LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
-    u32 nh = compact_indices(c, flag, list, e);
-    if (nh) {
-        u64 *tsz = c.arena.alloc<u64>(nh + 1);
-        LAUNCH(c, k_tab_sizes, cdiv(nh + 1, 256), 256, 0, list, nh, L.off, tsz);
-        scan_excl_u64(c, tsz, tsz, nh + 1);
-        u64 tot = fetch1(c, tsz + nh);
-        u32 *gtab = c.arena.alloc<u32>(4 * tot);
-        LAUNCH(c, k_census_block, nh, 512, 0, list, nh, A, gtab, (const u64 *)tsz);
+    cs.lam = c.arena.alloc<u32>(L.e ? L.e : 1);
+    return cs;
+}
+
+static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainArgs &A) {
+    fill_u32(c, A.target, NONE, L.n);
+    LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
+    LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, 2 * GN_BLOCK_W * 16, A, lp.ntier[1], lp.ncount[1], 2 * GN_BLOCK_W,
+           (u32 *)nullptr, lp.work);
+    if (lp.ncount[2]) {
+        size_t m = c.arena.mark();
+        u32 cap = 64;
+        while (cap < 2 * lp.heavy_work_max && cap < (1u << 28)) cap <<= 1;
+        u32 grid = lp.ncount[2] < (u32)c.sms * 2 ? lp.ncount[2] : (u32)c.sms * 2;
+        u32 *gtab = c.arena.alloc<u32>((u64)grid * 4 * cap);
+        LAUNCH(c, k_gain_block, grid, GN_BLOCK, 0, A, lp.ntier[2], lp.ncount[2], cap, gtab, lp.work);
+        c.arena.release(m);
     }
+}
+
+Census build_census(Ctx &c, const DLevel &L, const u32 *part) {
+    Census cs = alloc_census(c, L);
+    size_t m = c.arena.mark();
+    LevelPrep lp;
+    if (L.e) {
+        u32 *flag = c.arena.alloc<u32>(L.e);
+        lp.hblock = c.arena.alloc<u32>(L.e);
+        LAUNCH(c, k_flag_len, cdiv(L.e, 256), 256, 0, L.e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
+        lp.n_hblock = compact_indices(c, flag, lp.hblock, L.e);
+        lp.hhuge = c.arena.alloc<u32>(L.e);
+        LAUNCH(c, k_flag_len, cdiv(L.e, 256), 256, 0, L.e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
+        lp.n_hhuge = compact_indices(c, flag, lp.hhuge, L.e);
+        if (lp.n_hhuge) {
+            lp.huge_tab = c.arena.alloc<u64>(lp.n_hhuge + 1);
+            LAUNCH(c, k_tab_sizes, cdiv(lp.n_hhuge + 1, 256), 256, 0, lp.hhuge, lp.n_hhuge, L.off, lp.huge_tab);
+            scan_excl_u64(c, lp.huge_tab, lp.huge_tab, lp.n_hhuge + 1);
+            lp.huge_tot = fetch1(c, lp.huge_tab + lp.n_hhuge);
+        }
+    }
+    run_census(c, L, lp, part, cs);
     c.arena.release(m);
     return cs;
 }
@@ -820,189 +899,215 @@ void part_inbound(Ctx &c, const DLevel &L, const Census &cs, u64 *pinb, u32 K) {
 void refine_gains_only(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, const u32 *part,
                        u32 discount, u32 round, u32 *target, i64 *gain) {
     size_t m = c.arena.mark();
-    Census cs = build_census(c, L, part);
+    LevelPrep lp = prepare_level(c, L, wfx, rp.K);
+    Census cs = alloc_census(c, L);
+    run_census(c, L, lp, part, cs);
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
     part_sizes(c, L.n, part, L.nsize, psize, rp.K);
     part_inbound(c, L, cs, pinb, rp.K);
     GainArgs A = make_gain_args(L, wfx, rp, cs, part, psize, pinb, discount, round, target, gain, c.d_status);
-    run_gains(c, L, A);
+    run_gains(c, L, lp, A);
     check_status(c);
     c.arena.release(m);
 }
 
-// One round; returns true when moves were applied.
-static bool refine_round(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, u32 *part, u32 discount,
-                         u32 round) {
+// One round; returns true when moves were applied. One host round trip (the apply flag).
+static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
+                         u32 *part, u32 discount, u32 round) {
     const u32 n = L.n;
     size_t m0 = c.arena.mark();
-    Census cs = build_census(c, L, part);
+    Census cs = alloc_census(c, L);
+    run_census(c, L, lp, part, cs);
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
     part_sizes(c, n, part, L.nsize, psize, rp.K);
     part_inbound(c, L, cs, pinb, rp.K);
     u32 *target = c.arena.alloc<u32>(n);
     i64 *gain = c.arena.alloc<i64>(n);
     GainArgs A = make_gain_args(L, wfx, rp, cs, part, psize, pinb, discount, round, target, gain, c.d_status);
-    run_gains(c, L, A);
+    run_gains(c, L, lp, A);
+    // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
+    // [3] big cascade hyperedges
+    u32 *cnt = c.arena.alloc<u32>(8);
+    AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
+    u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3;
     // movers in id order, then ranked by (gain desc, id asc)
     u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n);
     LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag);
-    const u32 M = compact_indices(c, flag, mv, n);
-    if (M == 0) {
-        check_status(c);
-        c.arena.release(m0);
-        return false;
+    compact_indices_dn(c, flag, mv, n, dM);
+    const u32 kb = bits_for(lp.gain_bound);
+    u32 *khi = c.arena.alloc<u32>(n), *klo = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_move_keys, cdiv(n, 256), 256, 0, mv, dM, gain, lp.gain_bound, khi, klo);
+    if (kb > 32) {
+        // stable by the low word, then by the high word (a 64-bit LSD sort); the high words are
+        // recomputed for the permuted movers between the two passes
+        u32 *tmp = c.arena.alloc<u32>(n);
+        radix_sort_pairs_dn(c, klo, mv, dM, n, 32);
+        LAUNCH(c, k_move_keys, cdiv(n, 256), 256, 0, mv, dM, gain, lp.gain_bound, khi, tmp);
+        radix_sort_pairs_dn(c, khi, mv, dM, n, kb - 32);
+    } else {
+        radix_sort_pairs_dn(c, klo, mv, dM, n, kb);
     }
-    unsigned long long *gm = c.arena.alloc<unsigned long long>(1);
-    AXC_CUDA(cudaMemsetAsync(gm, 0, 8, c.stream));
-    LAUNCH(c, k_gain_max, cdiv(M, 256), 256, 0, mv, M, gain, gm);
-    const u64 gmax = fetch1(c, (const u64 *)gm);
-    const u32 kb = bits_for(gmax);
-    u32 *khi = c.arena.alloc<u32>(M), *klo = c.arena.alloc<u32>(M);
-    LAUNCH(c, k_move_keys, cdiv(M, 256), 256, 0, mv, M, gain, gmax, khi, klo);
-    if (kb > 32) radix_sort_pairs64(c, khi, klo, mv, M, kb - 32, 32);
-    else radix_sort_pairs(c, klo, mv, M, kb);
     u32 *rank = flag;
     fill_u32(c, rank, NONE, n);
-    LAUNCH(c, k_set_rank, cdiv(M, 256), 256, 0, mv, M, rank);
+    LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank);
     // cascade
     unsigned long long *g2 = c.arena.alloc<unsigned long long>(n);
     AXC_CUDA(cudaMemsetAsync(g2, 0, (size_t)n * 8, c.stream));
+    // inbound-set transitions (INCC): each destination pin of a mover gives at most two
+    const bool track = rp.delta < 0x7FFFFFFFu && lp.dst_pins;
+    const u64 tcap = track ? 2 * lp.dst_pins : 0;
+    u32 *tp = nullptr, *tr = nullptr;
+    int32_t *tdv = nullptr;
+    if (track) {
+        tp = c.arena.alloc<u32>(tcap);
+        tr = c.arena.alloc<u32>(tcap);
+        tdv = (int32_t *)c.arena.alloc<u32>(tcap);
+    }
     {
-        CascadeArgs C{L.e, rp.encourage ? 1 : 0, L.off, L.pins, wfx, cs.lam, cs.part, cs.cnt, rank, part, target, g2,
-                      c.d_status};
+        CascadeArgs C;
+        C.e = L.e; C.encourage = rp.encourage ? 1 : 0; C.off = L.off; C.pins = L.pins; C.nsrc = L.nsrc;
+        C.wfx = wfx; C.lam = cs.lam; C.cpart = cs.part; C.ccnt = cs.cnt; C.cdcnt = cs.dcnt; C.rank = rank;
+        C.part = part; C.target = target; C.g2 = g2;
+        C.track = track ? 1 : 0; C.tp = tp; C.tr = tr; C.tdv = tdv; C.dT = dT; C.tcap = tcap;
+        C.status = c.d_status;
         size_t m1 = c.arena.mark();
-        u32 *big = c.arena.alloc<u32>(L.e), *blist = c.arena.alloc<u32>(L.e);
-        AXC_CUDA(cudaMemsetAsync(big, 0, (size_t)L.e * 4, c.stream));
-        LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big);
-        u32 nb = compact_indices(c, big, blist, L.e);
-        if (nb) {
-            u64 *mvsz = c.arena.alloc<u64>(nb + 1), *tabsz = c.arena.alloc<u64>(nb + 1);
-            LAUNCH(c, k_big_sizes, cdiv(nb + 1, 256), 256, 0, blist, nb, L.off, cs.lam, mvsz, tabsz);
-            scan_excl_u64(c, mvsz, mvsz, nb + 1);
-            scan_excl_u64(c, tabsz, tabsz, nb + 1);
-            u64 t2[2];
-            t2[0] = fetch1(c, mvsz + nb);
-            t2[1] = fetch1(c, tabsz + nb);
-            u64 *smv = c.arena.alloc<u64>(t2[0] + 1);
-            u32 *stab = c.arena.alloc<u32>(t2[1] + 1);
-            LAUNCH(c, k_cascade_big, nb, 256, 0, C, blist, nb, smv, stab, mvsz, tabsz);
-        }
+        u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1);
+        if (L.e) LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
+        // scratch per resident block, sized by the level's largest hyperedge
+        const u64 mv_cap = lp.max_len ? lp.max_len : 1;
+        u64 cap = 32;
+        while (cap < 2 * (3 * mv_cap)) cap <<= 1;
+        const u32 grid = (u32)c.sms;
+        u64 *smv = c.arena.alloc<u64>((u64)grid * mv_cap);
+        u32 *stab = c.arena.alloc<u32>((u64)grid * 3 * cap);
+        if (L.e) LAUNCH(c, k_cascade_big, grid, 256, 0, C, big, dBig, smv, stab, mv_cap, 3 * cap);
         c.arena.release(m1);
     }
     // prefix gains in rank order
-    i64 *G = c.arena.alloc<i64>(M), *Gx = c.arena.alloc<i64>(M);
-    LAUNCH(c, k_gather_g2, cdiv(M, 256), 256, 0, mv, M, g2, Gx);
-    scan_excl_i64(c, Gx, G, M);
-    LAUNCH(c, k_incl_fix, cdiv(M, 256), 256, 0, Gx, G, M);
+    i64 *G = c.arena.alloc<i64>(n), *Gx = c.arena.alloc<i64>(n);
+    LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);
+    scan_excl_i64(c, Gx, G, n);
+    LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Gx, G, n);
     // size validity
-    i64 *Vs = c.arena.alloc<i64>(M);
-    AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)M * 8, c.stream));
+    i64 *Vs = c.arena.alloc<i64>(n);
+    AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)n * 8, c.stream));
     {
         size_t m1 = c.arena.mark();
-        const u32 ne = 2 * M;
-        u32 *key = c.arena.alloc<u32>(ne), *val = c.arena.alloc<u32>(ne);
-        LAUNCH(c, k_size_events, cdiv(ne, 256), 256, 0, mv, M, part, target, key, val);
-        radix_sort_pairs(c, key, val, ne, bits_for(rp.K ? rp.K - 1 : 0));
-        i64 *d = c.arena.alloc<i64>(ne), *E = c.arena.alloc<i64>(ne);
-        LAUNCH(c, k_size_delta, cdiv(ne, 256), 256, 0, mv, val, ne, L.nsize, d);
-        scan_excl_i64(c, d, E, ne);
-        LAUNCH(c, k_size_flags, cdiv(ne, 256), 256, 0, key, val, d, E, ne, psize, (u64)rp.omega,
+        const u32 nemax = 2 * n;
+        LAUNCH(c, k_twice, 1, 1, 0, dM, dSE);
+        u32 *key = c.arena.alloc<u32>(nemax), *val = c.arena.alloc<u32>(nemax);
+        LAUNCH(c, k_size_events, cdiv(nemax, 256), 256, 0, mv, dM, part, target, key, val);
+        radix_sort_pairs_dn(c, key, val, dSE, nemax, bits_for(rp.K ? rp.K - 1 : 0));
+        i64 *d = c.arena.alloc<i64>(nemax), *E = c.arena.alloc<i64>(nemax);
+        LAUNCH(c, k_size_delta, cdiv(nemax, 256), 256, 0, mv, val, dSE, nemax, L.nsize, d);
+        scan_excl_i64(c, d, E, nemax);
+        LAUNCH(c, k_size_flags, cdiv(nemax, 256), 256, 0, key, val, d, E, dSE, psize, (u64)rp.omega,
                (unsigned long long *)Vs);
         c.arena.release(m1);
     }
-    i64 *Vsx = c.arena.alloc<i64>(M);
-    scan_excl_i64(c, Vs, Vsx, M);
-    LAUNCH(c, k_incl_fix, cdiv(M, 256), 256, 0, Vs, Vsx, M);
+    i64 *Vsx = c.arena.alloc<i64>(n);
+    scan_excl_i64(c, Vs, Vsx, n);
+    LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Vs, Vsx, n);
     Vs = Vsx;
-    // inbound validity (INCC only)
+    // inbound validity (INCC only): the transitions ordered by (partition, rank), the running
+    // inbound-set size of each partition along them
     i64 *Vi = nullptr;
-    if (rp.delta < 0x7FFFFFFFu) {
-        Vi = c.arena.alloc<i64>(M);
-        AXC_CUDA(cudaMemsetAsync(Vi, 0, (size_t)M * 8, c.stream));
+    if (track) {
+        Vi = c.arena.alloc<i64>(n);
+        AXC_CUDA(cudaMemsetAsync(Vi, 0, (size_t)n * 8, c.stream));
         size_t m1 = c.arena.mark();
-        u32 *cnt = c.arena.alloc<u32>(M);
-        u64 *base = c.arena.alloc<u64>(M + 1);
-        LAUNCH(c, k_inb_counts, cdiv(M, 256), 256, 0, mv, M, L.nin, cnt);
-        offsets_from_counts(c, cnt, base, M);
-        const u64 ne = fetch1(c, base + M);
-        if (ne) {
-            u32 *keyH = c.arena.alloc<u32>(ne), *keyP = c.arena.alloc<u32>(ne), *val = c.arena.alloc<u32>(ne);
-            LAUNCH(c, k_inb_events, cdiv((u64)M * 32, 256), 256, 0, mv, M, base, L.toff, L.touch, L.nin, part, target,
-                   keyH, keyP, val);
-            radix_sort_pairs(c, keyH, val, ne, bits_for(L.e ? L.e - 1 : 0));
-            u32 *kp2 = c.arena.alloc<u32>(ne);
-            LAUNCH(c, k_gather_by, cdiv(ne, 256), 256, 0, keyP, val, kp2, ne);
-            radix_sort_pairs(c, kp2, val, ne, bits_for(rp.K ? rp.K - 1 : 0));
-            u32 *ev_h = keyH, *ev_r = keyP;  // reuse
-            i64 *ev_d = c.arena.alloc<i64>(ne);
-            u32 *head = c.arena.alloc<u32>(ne), *sid = c.arena.alloc<u32>(ne), *start = c.arena.alloc<u32>(ne);
-            LAUNCH(c, k_inb_decode, cdiv(ne, 256), 256, 0, val, kp2, ne, base, M, mv, L.toff, L.touch, ev_h, ev_r,
-                   ev_d, head);
-            LAUNCH(c, k_seg_heads, cdiv(ne, 256), 256, 0, kp2, ev_h, ne, head);
-            scan_excl_u32(c, head, sid, ne);
-            LAUNCH(c, k_seg_start, cdiv(ne, 256), 256, 0, head, sid, ne, start);
-            i64 *E = c.arena.alloc<i64>(ne);
-            scan_excl_i64(c, ev_d, E, ne);
-            u32 *tflag = c.arena.alloc<u32>(ne);
-            int32_t *tdelta = (int32_t *)c.arena.alloc<u32>(ne);
-            LAUNCH(c, k_inb_trans, cdiv(ne, 256), 256, 0, kp2, ev_h, ev_r, ev_d, E, head, sid, start, ne, L.off,
-                   cs.lam, cs.part, cs.dcnt, tflag, tdelta);
-            u32 *tidx = c.arena.alloc<u32>(ne);
-            const u32 T = compact_indices(c, tflag, tidx, ne);
-            if (T) {
-                u32 *tp = c.arena.alloc<u32>(T), *tr = c.arena.alloc<u32>(T), *perm = c.arena.alloc<u32>(T);
-                int32_t *td = (int32_t *)c.arena.alloc<u32>(T);
-                LAUNCH(c, k_trans_gather, cdiv(T, 256), 256, 0, tidx, T, kp2, ev_r, tdelta, tp, tr, td);
-                // order (p, r): stable by r, then stable by p
-                u32 *kr = c.arena.alloc<u32>(T), *kpp = c.arena.alloc<u32>(T);
-                AXC_CUDA(cudaMemcpyAsync(kr, tr, (size_t)T * 4, cudaMemcpyDeviceToDevice, c.stream));
-                LAUNCH(c, k_iota, cdiv(T, 256), 256, 0, perm, T);
-                radix_sort_pairs(c, kr, perm, T, bits_for(M - 1));
-                LAUNCH(c, k_gather_by, cdiv(T, 256), 256, 0, tp, perm, kpp, T);
-                radix_sort_pairs(c, kpp, perm, T, bits_for(rp.K ? rp.K - 1 : 0));
-                u32 *sr = kr;
-                i64 *sd = c.arena.alloc<i64>(T), *E2 = c.arena.alloc<i64>(T);
-                LAUNCH(c, k_trans_perm, cdiv(T, 256), 256, 0, perm, T, tr, td, sr, sd);
-                scan_excl_i64(c, sd, E2, T);
-                u32 *h2 = c.arena.alloc<u32>(T), *sid2 = c.arena.alloc<u32>(T), *st2 = c.arena.alloc<u32>(T);
-                LAUNCH(c, k_seg_heads, cdiv(T, 256), 256, 0, kpp, (const u32 *)nullptr, T, h2);
-                scan_excl_u32(c, h2, sid2, T);
-                LAUNCH(c, k_seg_start, cdiv(T, 256), 256, 0, h2, sid2, T, st2);
-                LAUNCH(c, k_trans_flags, cdiv(T, 256), 256, 0, kpp, sr, sd, E2, sid2, st2, T, pinb, (u64)rp.delta,
-                       (unsigned long long *)Vi);
-            }
+        const u64 nt = tcap;
+        const u32 rb = bits_for(n ? n - 1 : 0), pb = bits_for(rp.K ? rp.K - 1 : 0);
+        const bool combined = rb + pb <= 32;
+        LAUNCH(c, k_clamp_count, 1, 1, 0, dT, nt);  // an overflow already set the status word
+        u32 *key = c.arena.alloc<u32>(nt), *perm = c.arena.alloc<u32>(nt);
+        LAUNCH(c, k_trans_keys, cdiv(nt, 256), 256, 0, dT, nt, tp, tr, rb, combined ? 1 : 0, key, perm);
+        if (combined) {
+            radix_sort_pairs_dn(c, key, perm, dT, nt, rb + pb);
+        } else {
+            radix_sort_pairs_dn(c, key, perm, dT, nt, rb);
+            LAUNCH(c, k_gather_by_dn, cdiv(nt, 256), 256, 0, tp, perm, key, dT);
+            radix_sort_pairs_dn(c, key, perm, dT, nt, pb);
         }
+        u32 *sp = c.arena.alloc<u32>(nt), *sr = key;
+        i64 *sd = c.arena.alloc<i64>(nt), *E2 = c.arena.alloc<i64>(nt);
+        LAUNCH(c, k_trans_perm, cdiv(nt, 256), 256, 0, perm, dT, nt, tp, tr, tdv, sp, sr, sd);
+        scan_excl_i64(c, sd, E2, nt);
+        u32 *h2 = c.arena.alloc<u32>(nt), *sid2 = c.arena.alloc<u32>(nt), *st2 = c.arena.alloc<u32>(nt);
+        LAUNCH(c, k_seg_heads, cdiv(nt, 256), 256, 0, sp, (const u32 *)nullptr, dT, nt, h2);
+        scan_excl_u32(c, h2, sid2, nt);
+        LAUNCH(c, k_seg_start, cdiv(nt, 256), 256, 0, h2, sid2, dT, st2);
+        LAUNCH(c, k_trans_flags, cdiv(nt, 256), 256, 0, sp, sr, sd, E2, h2, sid2, st2, dT, pinb, (u64)rp.delta,
+               (unsigned long long *)Vi);
         c.arena.release(m1);
-        i64 *Vix = c.arena.alloc<i64>(M);
-        scan_excl_i64(c, Vi, Vix, M);
-        LAUNCH(c, k_incl_fix, cdiv(M, 256), 256, 0, Vi, Vix, M);
+        i64 *Vix = c.arena.alloc<i64>(n);
+        scan_excl_i64(c, Vi, Vix, n);
+        LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Vi, Vix, n);
         Vi = Vix;
     }
     // best prefix and apply
-    const u32 nbk = cdiv(M, 256) < 64u ? cdiv(M, 256) : 64u;
+    const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
     Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
     u32 *apply = c.arena.alloc<u32>(1);
-    LAUNCH(c, k_best, nbk, 256, 0, G, Vs, Vi, M, bb + 1);
+    LAUNCH(c, k_best, nbk, 256, 0, G, Vs, Vi, dM, bb + 1);
     LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, Vi, bb, apply);
-    LAUNCH(c, k_apply, cdiv(M, 256), 256, 0, mv, target, bb, apply, part);
-    const u32 applied = fetch1(c, apply);
-    check_status(c);
+    LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
+    // one round trip: the apply flag and the status word
+    AXC_CUDA(cudaMemcpyAsync(c.h_pinned, apply, 4, cudaMemcpyDeviceToHost, c.stream));
+    AXC_CUDA(cudaMemcpyAsync((char *)c.h_pinned + 4, c.d_status, 4, cudaMemcpyDeviceToHost, c.stream));
+    AXC_CUDA(cudaStreamSynchronize(c.stream));
+    u32 hv[2];
+    memcpy(hv, c.h_pinned, 8);
+    if (hv[1] != DEV_OK) {
+        AXC_CUDA(cudaMemsetAsync(c.d_status, 0, 4, c.stream));
+        throw Error(AXC_EINTERNAL, "device status word = " + std::to_string(hv[1]));
+    }
     c.arena.release(m0);
-    return applied != 0;
+    return hv[0] != 0;
+}
+
+// level bounds that need the offsets: the largest hyperedge and the destination pin count
+__global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
+                               unsigned long long *__restrict__ out) {
+    u32 h = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 len = 0, dst = 0;
+    if (h < e) {
+        len = off[h + 1] - off[h];
+        dst = len - nsrc[h];
+    }
+    len = warp_max_u64(len);
+    dst = warp_sum(dst);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], (unsigned long long)len);
+        atomicAdd(&out[1], (unsigned long long)dst);
+    }
 }
 
 u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, u32 *part) {
     const u32 R = rp.rounds;
+    if (R == 0 || L.n == 0) return 0;
+    size_t m = c.arena.mark();
+    LevelPrep lp = prepare_level(c, L, wfx, rp.K);
+    {
+        unsigned long long *b = c.arena.alloc<unsigned long long>(2);
+        AXC_CUDA(cudaMemsetAsync(b, 0, 16, c.stream));
+        if (L.e) LAUNCH(c, k_level_bounds, cdiv(L.e, 256), 256, 0, L.e, L.off, L.nsrc, b);
+        u64 h[2];
+        fetch(c, h, b, 16);
+        lp.max_len = h[0];
+        lp.dst_pins = h[1];
+    }
     u32 done = 0;
     for (u32 r = 0; r < R; ++r) {
         const u32 discount = r < R / 3 ? 1u : (r < 2 * R / 3 ? 2u : 0xFFFFFFFFu);
         ++done;
-        if (!refine_round(c, L, wfx, rp, part, discount, r)) {
+        if (!refine_round(c, L, lp, wfx, rp, part, discount, r)) {
             if (r < R / 3) r = R / 2;
             else if (r < 2 * R / 3) r = 2 * R / 3;
             else r = R;
         }
     }
+    c.arena.release(m);
     return done;
 }
 

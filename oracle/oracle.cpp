@@ -152,18 +152,26 @@ void rating(const G &g, const std::vector<u32> &wfx, const T &t, const u32 *nsiz
     }
 }
 
-// Deterministic matching. Rounds of mutual proposals: every unmatched node proposes to its best
-// still-unmatched candidate (candidate lists are in (score desc, id desc) order); mutual proposals
-// match. All reads in a round see the previous round's state. Stops at a fixed point or after
-// `rounds`. Orphans (nodes without any candidate) are then paired k-th smallest with k-th largest
-// by (size, id) when size and inbound-count sums fit (sources/chaining.cu:260-329,
+// Deterministic matching by rounds of proposals (this build's rule; the reference's
+// grouping_kernel, kernels/coarsening.cu:241-505, resolves its candidate forests with atomics).
+// Each round, on the previous round's state:
+//  A. every unmatched node u proposes to its best still-unmatched candidate p(u) (candidate lists
+//     are in (score desc, id desc) order);
+//  B. every node v accepts its best proposer best(v) by (score, id);
+//  C. with acc(u) = [best(p(u)) == u]: u and p(u) match when acc(u) and not acc(p(u)) (p(u)'s own
+//     proposal was refused, so it is free), or when they propose to and accept each other.
+// Each node is matched at most once per round. Stops at a fixed point or after `rounds`.
+// Orphans (nodes without any candidate) are then paired k-th smallest with k-th largest by
+// (size, id) when size and inbound-count sums fit (sources/chaining.cu:260-329,
 // kernels/chaining.cu:237-270). Groups are relabelled 0.. in order of their smallest member.
-u32 matching(u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u32 *nin, u32 omega,
-             u32 delta, u32 rounds, u32 *groups) {
+u32 matching(u32 n, u32 cnc, const u32 *pairs, const u32 *scores, const u32 *nsize, const u32 *nin,
+             u32 omega, u32 delta, u32 rounds, u32 *groups) {
     std::vector<u32> mate(n, NONE), ptr(n, 0), prop(n, NONE);
+    std::vector<u64> best(n, 0);
     for (u32 r = 0; r < rounds; ++r) {
         for (u32 v = 0; v < n; ++v) {
             prop[v] = NONE;
+            best[v] = 0;
             if (mate[v] != NONE) continue;
             u32 p = ptr[v];
             while (p < cnc) {
@@ -175,12 +183,44 @@ u32 matching(u32 n, u32 cnc, const u32 *pairs, const u32 *nsize, const u32 *nin,
             ptr[v] = p;
             if (p < cnc) prop[v] = pairs[(u64)v * cnc + p];
         }
+        for (u32 u = 0; u < n; ++u)
+            if (prop[u] != NONE) {
+                u64 key = ((u64)scores[(u64)u * cnc + ptr[u]] << 32) | u;
+                best[prop[u]] = std::max(best[prop[u]], key);
+            }
+        // candidate scores are > 0, so a node with proposers has best != 0
+        auto acc = [&](u32 u) { return prop[u] != NONE && best[prop[u]] != 0 && (u32)best[prop[u]] == u; };
         bool changed = false;
-        for (u32 v = 0; v < n; ++v) {
-            u32 w = prop[v];
-            if (w != NONE && w > v && prop[w] == v) { mate[v] = w; mate[w] = v; changed = true; }
+        std::vector<std::pair<u32, u32>> mk;
+        for (u32 u = 0; u < n; ++u) {
+            const u32 v = prop[u];
+            if (v == NONE || !acc(u)) continue;
+            const bool av = acc(v);
+            if (!av || (prop[v] == u && u < v)) mk.push_back({u, v});
         }
+        for (auto &x : mk) { mate[x.first] = x.second; mate[x.second] = x.first; changed = true; }
         if (!changed) break;
+    }
+    // Two-hop pass: still-unmatched nodes that have candidates are bucketed by their best
+    // candidate; within a bucket (ascending ids) positions 2i and 2i+1 pair up when their size sum
+    // fits omega and their inbound-count sum fits delta.
+    {
+        std::vector<std::pair<u32, u32>> hop;  // (best candidate, node)
+        for (u32 v = 0; v < n; ++v)
+            if (mate[v] == NONE && pairs[(u64)v * cnc] != NONE) hop.push_back({pairs[(u64)v * cnc], v});
+        std::sort(hop.begin(), hop.end());
+        size_t i = 0;
+        while (i < hop.size()) {
+            size_t j = i;
+            while (j < hop.size() && hop[j].first == hop[i].first) ++j;
+            for (size_t a = i; a + 1 < j; a += 2) {
+                const u32 x = hop[a].second, y = hop[a + 1].second;
+                if ((u64)nsize[x] + nsize[y] > omega || (u64)nin[x] + nin[y] > delta) continue;
+                mate[x] = y;
+                mate[y] = x;
+            }
+            i = j;
+        }
     }
     std::vector<u32> orph;
     for (u32 v = 0; v < n; ++v)
@@ -675,10 +715,10 @@ void or_rating(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins
     rating(g, w, t, node_size, omega, delta, cnc, pairs, scores);
 }
 
-uint32_t or_matching(uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *node_size,
-                     const uint32_t *inbound, uint32_t omega, uint32_t delta, uint32_t rounds,
-                     uint32_t *groups) {
-    return matching(n, cnc, pairs, node_size, inbound, omega, delta, rounds, groups);
+uint32_t or_matching(uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *scores,
+                     const uint32_t *node_size, const uint32_t *inbound, uint32_t omega, uint32_t delta,
+                     uint32_t rounds, uint32_t *groups) {
+    return matching(n, cnc, pairs, scores, node_size, inbound, omega, delta, rounds, groups);
 }
 
 uint64_t or_contract(uint32_t e, const uint64_t *off, const uint32_t *pins, const uint32_t *nsrc,
@@ -783,7 +823,7 @@ uint32_t or_partition(uint32_t n, uint32_t e, const uint64_t *off, const uint32_
         std::vector<u32> pairs((size_t)cn * cnc), scores((size_t)cn * cnc), groups(cn);
         rating(cur.g, wfx, cur.t, cur.nsize.data(), kway ? omega_c : omega, delta, cnc,
                pairs.data(), scores.data());
-        u32 ng = matching(cn, cnc, pairs.data(), cur.nsize.data(), cur.t.nin.data(),
+        u32 ng = matching(cn, cnc, pairs.data(), scores.data(), cur.nsize.data(), cur.t.nin.data(),
                           kway ? omega_c : omega, delta, 32, groups.data());
         const float ratio = (float)ng / (float)cn;
         if (kway && (ratio > 0.95f || ng < 1024)) {

@@ -40,11 +40,11 @@ void or_rating(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins
                const uint32_t *touch, const uint32_t *inbound, const uint32_t *node_size,
                uint32_t omega, uint32_t delta, uint32_t cnc, uint32_t *pairs, uint32_t *scores);
 
-/* Matching + orphan pairing + relabel (this build's deterministic mutual-proposal matching;
+/* Matching + orphan pairing + relabel (this build's deterministic propose/accept matching;
  * orphans as sources/chaining.cu:260-329). Returns the number of groups. */
-uint32_t or_matching(uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *node_size,
-                     const uint32_t *inbound, uint32_t omega, uint32_t delta, uint32_t rounds,
-                     uint32_t *groups);
+uint32_t or_matching(uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *scores,
+                     const uint32_t *node_size, const uint32_t *inbound, uint32_t omega, uint32_t delta,
+                     uint32_t rounds, uint32_t *groups);
 
 /* Contraction, kernels/construction.cu:304-489. Returns the coarse pin count. */
 uint64_t or_contract(uint32_t e, const uint64_t *off, const uint32_t *pins, const uint32_t *nsrc,

@@ -99,12 +99,13 @@ def rating(n, off, pins, nsrc, wfx_, node_size, omega, delta, cnc):
     return pairs[: n * cnc], scores[: n * cnc]
 
 
-def matching(n, cnc, pairs, node_size, inbound, omega, delta, rounds=32):
-    pairs, ns, nin = _u32(pairs), _u32(node_size), _u32(inbound)
+def matching(n, cnc, pairs, scores, node_size, inbound, omega, delta, rounds=32):
+    pairs, scores, ns, nin = _u32(pairs), _u32(scores), _u32(node_size), _u32(inbound)
     groups = np.zeros(max(n, 1), np.uint32)
     L = lib()
     L.or_matching.restype = C.c_uint32
-    ng = L.or_matching(C.c_uint32(n), C.c_uint32(cnc), _p(pairs, C.c_uint32), _p(ns, C.c_uint32),
+    ng = L.or_matching(C.c_uint32(n), C.c_uint32(cnc), _p(pairs, C.c_uint32), _p(scores, C.c_uint32),
+                       _p(ns, C.c_uint32),
                        _p(nin, C.c_uint32), C.c_uint32(omega), C.c_uint32(delta), C.c_uint32(rounds),
                        _p(groups, C.c_uint32))
     return groups[:n], ng

@@ -103,9 +103,22 @@ def test_matching_matches_oracle(ctx, name, cnc):
     g = dedup(golden(name))
     ns = np.ones(g.n, np.uint32)
     toff, touch, nin = O.touching(g.n, g.off, g.pins, g.nsrc)
-    pairs, _ = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 1 << 20, 1 << 20, cnc)
-    groups, ng = ctx.stage_matching(g.n, cnc, pairs, ns, nin, 1 << 20, 1 << 20)
-    o_groups, o_ng = O.matching(g.n, cnc, pairs, ns, nin, 1 << 20, 1 << 20)
+    pairs, scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 1 << 20, 1 << 20, cnc)
+    groups, ng = ctx.stage_matching(g.n, cnc, pairs, scores, ns, nin, 1 << 20, 1 << 20)
+    o_groups, o_ng = O.matching(g.n, cnc, pairs, scores, ns, nin, 1 << 20, 1 << 20)
+    assert ng == o_ng
+    np.testing.assert_array_equal(groups, o_groups)
+
+
+@pytest.mark.parametrize("wl", ["snn-8x512", "circuit-200k-k2"])
+def test_matching_full_size(ctx, wl):
+    g, _ = ax.workload(wl)
+    g = dedup(g)
+    ns = np.ones(g.n, np.uint32)
+    toff, touch, nin = O.touching(g.n, g.off, g.pins, g.nsrc)
+    pairs, scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 1 << 20, 0x7FFFFFFF, 4)
+    groups, ng = ctx.stage_matching(g.n, 4, pairs, scores, ns, nin, 1 << 20, 0x7FFFFFFF)
+    o_groups, o_ng = O.matching(g.n, 4, pairs, scores, ns, nin, 1 << 20, 0x7FFFFFFF)
     assert ng == o_ng
     np.testing.assert_array_equal(groups, o_groups)
 
@@ -114,10 +127,11 @@ def test_matching_orphans(ctx):
     # no candidates at all: everything is an orphan; pairing by (size, id) under omega and delta
     n, cnc = 11, 2
     pairs = np.full(n * cnc, NONE, np.uint32)
+    scores = np.zeros(n * cnc, np.uint32)
     ns = np.array([3, 1, 4, 1, 5, 9, 2, 6, 5, 3, 5], np.uint32)
     nin = np.array([1, 0, 2, 7, 1, 0, 3, 1, 2, 0, 1], np.uint32)
-    groups, ng = ctx.stage_matching(n, cnc, pairs, ns, nin, 10, 5)
-    o_groups, o_ng = O.matching(n, cnc, pairs, ns, nin, 10, 5)
+    groups, ng = ctx.stage_matching(n, cnc, pairs, scores, ns, nin, 10, 5)
+    o_groups, o_ng = O.matching(n, cnc, pairs, scores, ns, nin, 10, 5)
     assert ng == o_ng
     np.testing.assert_array_equal(groups, o_groups)
 
