@@ -64,6 +64,11 @@ class Stats(C.Structure):
     ]
 
 
+class KernelTiming(C.Structure):
+    """axc_kernel_timing: launches, summed event-timed duration and algorithmic bytes of one kernel."""
+    _fields_ = [("launches", C.c_uint32), ("ms_total", C.c_double), ("bytes", C.c_uint64)]
+
+
 # Every symbol include/axc.h declares (tests check the library exports all of them).
 EXPORTS = [
     "axc_create", "axc_destroy", "axc_strerror", "axc_last_error", "axc_params_default",
@@ -72,7 +77,7 @@ EXPORTS = [
     "axc_write_hgraph", "axc_write_partition", "axc_read_partition", "axc_quotient_hgraph",
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
-    "axc_stage_gains",
+    "axc_stage_gains", "axc_profile_kernel", "axc_profile_read",
 ]
 
 _lib = None
@@ -122,6 +127,8 @@ def lib() -> C.CDLL:
             "axc_stage_gains": (C.c_int, [C.c_void_p, H, u32p, C.c_uint32, u32p, C.c_uint32, C.c_uint32,
                                           C.c_int, C.c_uint32, u32p, i64p]),
         }
+        sig["axc_profile_kernel"] = (C.c_int, [C.c_void_p, C.c_char_p])
+        sig["axc_profile_read"] = (C.c_int, [C.c_void_p, C.POINTER(KernelTiming)])
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res
@@ -259,6 +266,16 @@ class Context:
     def _check(self, rc: int, what: str):
         if rc:
             raise AxcError(rc, f"{what}: {lib().axc_last_error(self._h).decode(errors='replace')}")
+
+    def profile_kernel(self, name: str | None):
+        """Time every launch of the named kernel with CUDA events on the context stream."""
+        self._check(lib().axc_profile_kernel(self._h, name.encode() if name else None), "axc_profile_kernel")
+
+    def profile_read(self) -> KernelTiming:
+        """Launches, summed duration (ms) and algorithmic bytes since the last read; resets them."""
+        t = KernelTiming()
+        self._check(lib().axc_profile_read(self._h, C.byref(t)), "axc_profile_read")
+        return t
 
     def partition(self, g: Hypergraph, p: Params) -> tuple[np.ndarray, Stats]:
         out = np.zeros(max(g.n, 1), np.uint32)

@@ -24,6 +24,18 @@ enum DevStatus : u32 {
     DEV_OK = 0,
     DEV_HASH_FULL = 1,      // a bounded hash table could not take a key
     DEV_BAD_INDEX = 2,      // an index check failed
+    DEV_SPIN_LIMIT = 3,     // a bounded wait gave up (a predecessor tile never published)
+};
+
+// Tile states of the single-pass scans: per tile a flag (epoch << 2 | 1 aggregate, 2 inclusive)
+// and two values, kept for the context's lifetime so no scan has to clear them. ctrl[0] hands
+// out tiles in launch order, ctrl[1] counts finished tiles and ctrl[2] is the launch's epoch: the
+// last tile to finish resets the first two and advances the epoch, all on the device.
+struct ScanState {
+    u32 *flag = nullptr;
+    u64 *agg = nullptr, *incl = nullptr;
+    u32 *ctrl = nullptr;
+    u32 cap_tiles = 0;
 };
 
 struct Error : std::runtime_error {
@@ -71,17 +83,21 @@ struct Ctx {
     u32 launches = 0;
     std::string last_error;
     int coop_supported = 0;
+    ScanState scan;
     // Kernel timer: while on, every launch of the kernel named `prof_name` is bracketed by a pair
-    // of events on the context stream; kernels with a byte model add their algorithmic bytes to
-    // prof_dbytes (device) or prof_hbytes (host).
+    // of events on the context stream; launch sites with a byte model add the launch's
+    // algorithmic bytes to prof_bytes.
+    // Pairs recorded inside a CUDA graph capture become event-record nodes; the code that
+    // replays the graph adds their durations to prof_ms / prof_launches after each replay.
     bool prof_on = false;
     std::string prof_name;
     std::vector<cudaEvent_t> prof_ev;
     size_t prof_used = 0;
-    u64 *prof_dbytes = nullptr;
-    u64 prof_hbytes = 0;
+    u64 prof_bytes = 0;
+    double prof_ms = 0;
+    u32 prof_launches = 0;
+    bool capturing = false;
     bool profiling(const char *name) const { return prof_on && prof_name == name; }
-    u64 *prof_counter(const char *name) const { return profiling(name) ? prof_dbytes : nullptr; }
     cudaEvent_t prof_event() {
         if (prof_used == prof_ev.size()) {
             cudaEvent_t e;
@@ -89,6 +105,20 @@ struct Ctx {
             prof_ev.push_back(e);
         }
         return prof_ev[prof_used++];
+    }
+    void prof_record(cudaEvent_t e) {
+        if (capturing) cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal);
+        else cudaEventRecord(e, stream);
+    }
+    // Adds the durations of the recorded pairs [from, to) (their work must have completed).
+    void prof_collect(size_t from, size_t to) {
+        for (size_t i = from; i + 1 < to; i += 2) {
+            float t = 0;
+            if (cudaEventElapsedTime(&t, prof_ev[i], prof_ev[i + 1]) == cudaSuccess) {
+                prof_ms += t;
+                prof_launches++;
+            }
+        }
     }
 };
 
@@ -99,13 +129,13 @@ struct Ctx {
         if ((grid) > 0) {                                                                      \
             const bool _prof = (ctx).profiling(#kern);                                         \
             cudaEvent_t _e0 = _prof ? (ctx).prof_event() : nullptr;                           \
-            if (_e0) cudaEventRecord(_e0, (ctx).stream);                                       \
+            if (_e0) (ctx).prof_record(_e0);                                                   \
             kern<<<(grid), (block), (smem), (ctx).stream>>>(__VA_ARGS__);                      \
             (ctx).launches++;                                                                  \
             AXC_CUDA(cudaGetLastError());                                                      \
             if (_e0) {                                                                         \
                 cudaEvent_t _e1 = (ctx).prof_event();                                          \
-                if (_e1) cudaEventRecord(_e1, (ctx).stream);                                   \
+                if (_e1) (ctx).prof_record(_e1);                                               \
                 else (ctx).prof_used--;                                                        \
             }                                                                                  \
         }                                                                                      \
@@ -214,6 +244,10 @@ __device__ __forceinline__ u32 hash_find(const u32 *keys, u32 mask, u32 key) {
 void scan_excl_u32(Ctx &c, const u32 *in, u32 *out, u64 n);
 void scan_excl_u64(Ctx &c, const u64 *in, u64 *out, u64 n);
 void scan_excl_i64(Ctx &c, const i64 *in, i64 *out, u64 n);
+void scan_incl_i64(Ctx &c, const i64 *in, i64 *out, u64 n);
+// Tile state of the single-pass scans (made by axc_create, freed by axc_destroy).
+void scan_state_create(Ctx &c, u32 cap_tiles);
+void scan_state_destroy(Ctx &c);
 // u32 counts -> u64 exclusive offsets with out[n] = total (out has n+1 entries)
 void offsets_from_counts(Ctx &c, const u32 *counts, u64 *out, u64 n);
 // Stable LSD radix sort of (key, value) pairs by the low `bits` bits of key. In place: on

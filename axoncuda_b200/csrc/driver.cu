@@ -279,6 +279,7 @@ int axc_create(int device, size_t arena_bytes, axc_ctx **out) {
         setup_construct_kernels();
         setup_coarsen_kernels(c);
         setup_refine_kernels(c);
+        scan_state_create(c, 1u << 18);  // single-pass scans of up to 2^29 elements
         AXC_CUDA(cudaDeviceSynchronize());
     } catch (const std::exception &e) {
         int rc = guard(x, e);
@@ -289,14 +290,49 @@ int axc_create(int device, size_t arena_bytes, axc_ctx **out) {
     return AXC_OK;
 }
 
+int axc_profile_kernel(axc_ctx *ctx, const char *kernel) {
+    if (!ctx) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Ctx &c = ctx->c;
+    c.prof_on = kernel != nullptr;
+    c.prof_name = kernel ? kernel : "";
+    c.prof_used = 0;
+    c.prof_bytes = 0;
+    c.prof_ms = 0;
+    c.prof_launches = 0;
+    return AXC_OK;
+}
+
+int axc_profile_read(axc_ctx *ctx, axc_kernel_timing *out) {
+    if (!ctx || !out) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Ctx &c = ctx->c;
+    try {
+        AXC_CUDA(cudaStreamSynchronize(c.stream));
+        c.prof_collect(0, c.prof_used);
+        out->launches = c.prof_launches;
+        out->ms_total = c.prof_ms;
+        out->bytes = c.prof_bytes;
+        c.prof_used = 0;
+        c.prof_bytes = 0;
+        c.prof_ms = 0;
+        c.prof_launches = 0;
+    } catch (const std::exception &e) {
+        return guard(ctx, e);
+    }
+    return AXC_OK;
+}
+
 void axc_destroy(axc_ctx *ctx) {
     if (!ctx) return;
     Ctx &c = ctx->c;
     extern void axc_batch_free(axc_ctx *);
     axc_batch_free(ctx);
     if (c.stream) cudaStreamSynchronize(c.stream);
+    for (cudaEvent_t e : c.prof_ev) cudaEventDestroy(e);
     if (c.arena.base) cudaFree(c.arena.base);
     if (c.d_status) cudaFree(c.d_status);
+    scan_state_destroy(c);
     if (c.h_pinned) cudaFreeHost(c.h_pinned);
     if (c.stream) cudaStreamDestroy(c.stream);
     delete ctx;

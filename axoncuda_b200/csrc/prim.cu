@@ -1,6 +1,7 @@
-// Device primitives owned by the library (no Thrust/CUB): exclusive scans (reduce-then-scan over
-// 2048-element tiles), a stable LSD radix sort with warp-level match_any ranking, stable index
-// compaction, fills and reductions. Every launch goes through the context's stream.
+// Device primitives owned by the library (no Thrust/CUB): single-pass scans and compaction
+// (decoupled look-back over 2048-element tiles, Merrill & Garland 2016), a stable LSD radix sort
+// with warp-level match_any ranking, fills and reductions. Every launch goes through the
+// context's stream.
 #include "common.cuh"
 
 namespace axc {
@@ -90,10 +91,180 @@ __global__ void k_tile_scan(const TI *__restrict__ in, TO *__restrict__ out, con
     }
 }
 
-template <class TI, class TO>
+// ------------------------------------------------------------------ single-pass look-back
+constexpr u32 LB_SPIN_LIMIT = 1u << 24;  // polls of one predecessor flag before giving up
+
+__device__ __forceinline__ u32 ld_flag(const u32 *p) { return *(const volatile u32 *)p; }
+
+// Tile ticket and epoch of this block (every thread gets both).
+__device__ __forceinline__ u32 lb_enter(const ScanState &S, u32 &s_tile, u32 &s_epoch, u32 &epoch) {
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(&S.ctrl[0], 1u);
+        s_epoch = *(volatile u32 *)&S.ctrl[2];
+    }
+    __syncthreads();
+    epoch = s_epoch;
+    return s_tile;
+}
+// The last block of the launch to finish resets the ticket and finish counters and advances the
+// epoch for the next launch (every block has taken its ticket by then).
+__device__ __forceinline__ void lb_leave(const ScanState &S, u32 epoch) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&S.ctrl[1], 1u) == gridDim.x - 1) {
+            S.ctrl[0] = 0;
+            S.ctrl[1] = 0;
+            __threadfence();
+            atomicExch(&S.ctrl[2], epoch + 1 < (1u << 30) ? epoch + 1 : 1u);
+        }
+    }
+}
+
+// Tiles take tickets in launch order, so a tile only ever waits on tiles already running. Each
+// tile publishes its aggregate, then (after looking back over its predecessors with warp 0) its
+// inclusive prefix. Returns the exclusive prefix of the tile to every thread.
+template <class TO>
+__device__ TO lookback_prefix(const ScanState &S, u32 epoch, u32 t, TO tile_total, u32 *status, TO *s_prefix) {
+    const u32 lane = threadIdx.x & 31u;
+    if (threadIdx.x == 0) {
+        if (t == 0) {
+            S.incl[0] = (u64)tile_total;
+            __threadfence();
+            atomicExch(&S.flag[0], (epoch << 2) | 2u);
+        } else {
+            S.agg[t] = (u64)tile_total;
+            __threadfence();
+            atomicExch(&S.flag[t], (epoch << 2) | 1u);
+        }
+    }
+    if (t > 0 && threadIdx.x < 32) {
+        TO excl = 0;
+        long long j = (long long)t - 1;
+        bool gave_up = false;
+        while (j >= 0) {
+            const long long idx = j - (long long)lane;
+            u32 st = 0;
+            u64 v = 0;
+            if (idx >= 0) {
+                u32 f = 0;
+                for (u32 it = 0;; ++it) {
+                    f = ld_flag(&S.flag[idx]);
+                    if ((f >> 2) == epoch && (f & 3u)) break;
+                    if (it >= LB_SPIN_LIMIT) {
+                        gave_up = true;
+                        f = (epoch << 2) | 2u;
+                        break;
+                    }
+                    if (it > 64) __nanosleep(64);
+                }
+                __threadfence();
+                st = f & 3u;
+                v = gave_up ? 0 : (st == 2u ? *(volatile u64 *)&S.incl[idx] : *(volatile u64 *)&S.agg[idx]);
+            }
+            const u32 inc = __ballot_sync(0xFFFFFFFFu, idx >= 0 && st == 2u);
+            if (inc) {
+                const u32 k = __ffs(inc) - 1;
+                excl += warp_sum<TO>(lane <= k ? (TO)v : TO(0));
+                break;
+            }
+            excl += warp_sum<TO>((TO)v);
+            j -= 32;
+        }
+        if (__any_sync(0xFFFFFFFFu, gave_up) && lane == 0) atomicExch(status, (u32)DEV_SPIN_LIMIT);
+        if (lane == 0) {
+            S.incl[t] = (u64)(excl + tile_total);
+            __threadfence();
+            atomicExch(&S.flag[t], (epoch << 2) | 2u);
+            *s_prefix = excl;
+        }
+    }
+    __syncthreads();
+    return t > 0 ? *s_prefix : TO(0);
+}
+
+// Scan: out[i] = sum of in[0..i) (exclusive) or in[0..i] (inclusive), in one pass.
+template <class TI, class TO, bool INCL>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_lb(const TI *__restrict__ in, TO *__restrict__ out, u64 n,
+                                                        ScanState S, u32 *status) {
+    __shared__ TO wt[33];
+    __shared__ TO stage[SCAN_TILE + SCAN_TILE / 32];
+    __shared__ u32 s_tile, s_epoch;
+    __shared__ TO s_prefix;
+    u32 epoch;
+    const u32 t = lb_enter(S, s_tile, s_epoch, epoch);
+    const u64 base = (u64)t * SCAN_TILE;
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = j * SCAN_THREADS + threadIdx.x;
+        u64 i = base + li;
+        stage[li + li / 32] = i < n ? (TO)in[i] : TO(0);
+    }
+    __syncthreads();
+    TO loc[SCAN_ITEMS];
+    TO s = 0;
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = threadIdx.x * SCAN_ITEMS + j;
+        loc[j] = stage[li + li / 32];
+        s += loc[j];
+    }
+    TO tot;
+    TO pre = block_excl_scan<TO>(s, wt, tot);
+    pre += lookback_prefix<TO>(S, epoch, t, tot, status, &s_prefix);
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = threadIdx.x * SCAN_ITEMS + j;
+        stage[li + li / 32] = INCL ? pre + loc[j] : pre;
+        pre += loc[j];
+    }
+    __syncthreads();
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        int li = j * SCAN_THREADS + threadIdx.x;
+        u64 i = base + li;
+        if (i < n) out[i] = stage[li + li / 32];
+    }
+    lb_leave(S, epoch);
+}
+
+// Stable compaction: out[k] = the k-th index i < n with flags[i] != 0; *total = their count.
+__global__ void __launch_bounds__(SCAN_THREADS) k_compact_lb(const u32 *__restrict__ flags, u32 *__restrict__ out,
+                                                           u64 n, u32 *__restrict__ total, ScanState S,
+                                                           u32 *status) {
+    __shared__ u32 wt[33];
+    __shared__ u32 s_tile, s_epoch;
+    __shared__ u32 s_prefix;
+    u32 epoch;
+    const u32 t = lb_enter(S, s_tile, s_epoch, epoch);
+    // thread-contiguous items: thread k owns elements [base + k*ITEMS, base + (k+1)*ITEMS)
+    const u64 base = (u64)t * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
+    u32 f[SCAN_ITEMS], s = 0;
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        u64 i = base + j;
+        f[j] = (i < n && flags[i]) ? 1u : 0u;
+        s += f[j];
+    }
+    u32 tot;
+    u32 pre = block_excl_scan<u32>(s, wt, tot);
+    pre += lookback_prefix<u32>(S, epoch, t, tot, status, &s_prefix);
+#pragma unroll
+    for (int j = 0; j < SCAN_ITEMS; ++j) {
+        if (f[j]) out[pre] = (u32)(base + j);
+        pre += f[j];
+    }
+    if (base < n && base + SCAN_ITEMS >= n) *total = pre;  // the thread holding element n-1
+    lb_leave(S, epoch);
+}
+
+template <class TI, class TO, bool INCL = false>
 void scan_impl(Ctx &c, const TI *in, TO *out, u64 n) {
     if (n == 0) return;
     const u32 tiles = cdiv(n, SCAN_TILE);
+    if (tiles <= c.scan.cap_tiles) {
+        LAUNCH(c, (k_scan_lb<TI, TO, INCL>), tiles, SCAN_THREADS, 0, in, out, n, c.scan, c.d_status);
+        return;
+    }
+    if (INCL) throw Error(AXC_EOVERFLOW, "inclusive scan longer than the look-back tile state");
     if (tiles == 1) {
         LAUNCH(c, (k_tile_scan<TI, TO>), 1, SCAN_THREADS, 0, in, out, (const TO *)nullptr, n);
         return;
@@ -235,6 +406,27 @@ inline u32 grid_for(Ctx &c, u64 n, u32 threads = 256) {
 void scan_excl_u32(Ctx &c, const u32 *in, u32 *out, u64 n) { scan_impl<u32, u32>(c, in, out, n); }
 void scan_excl_u64(Ctx &c, const u64 *in, u64 *out, u64 n) { scan_impl<u64, u64>(c, in, out, n); }
 void scan_excl_i64(Ctx &c, const i64 *in, i64 *out, u64 n) { scan_impl<i64, i64>(c, in, out, n); }
+void scan_incl_i64(Ctx &c, const i64 *in, i64 *out, u64 n) { scan_impl<i64, i64, true>(c, in, out, n); }
+
+void scan_state_create(Ctx &c, u32 cap_tiles) {
+    ScanState &S = c.scan;
+    AXC_CUDA(cudaMalloc(&S.flag, (size_t)cap_tiles * 4));
+    AXC_CUDA(cudaMalloc(&S.agg, (size_t)cap_tiles * 8));
+    AXC_CUDA(cudaMalloc(&S.incl, (size_t)cap_tiles * 8));
+    AXC_CUDA(cudaMalloc(&S.ctrl, 16));
+    AXC_CUDA(cudaMemset(S.flag, 0, (size_t)cap_tiles * 4));
+    const u32 ctrl0[4] = {0, 0, 1, 0};  // epoch 1: no flag carries it yet
+    AXC_CUDA(cudaMemcpy(S.ctrl, ctrl0, 16, cudaMemcpyHostToDevice));
+    S.cap_tiles = cap_tiles;
+}
+void scan_state_destroy(Ctx &c) {
+    ScanState &S = c.scan;
+    if (S.flag) cudaFree(S.flag);
+    if (S.agg) cudaFree(S.agg);
+    if (S.incl) cudaFree(S.incl);
+    if (S.ctrl) cudaFree(S.ctrl);
+    S = ScanState();
+}
 
 void offsets_from_counts(Ctx &c, const u32 *counts, u64 *out, u64 n) {
     if (n) scan_impl<u32, u64>(c, counts, out, n);
@@ -291,6 +483,11 @@ void compact_indices_dn(Ctx &c, const u32 *flags, u32 *out, u64 n, u32 *d_count)
         AXC_CUDA(cudaMemsetAsync(d_count, 0, 4, c.stream));
         return;
     }
+    const u32 tiles = cdiv(n, SCAN_TILE);
+    if (tiles <= c.scan.cap_tiles) {
+        LAUNCH(c, k_compact_lb, tiles, SCAN_THREADS, 0, flags, out, n, d_count, c.scan, c.d_status);
+        return;
+    }
     size_t m = c.arena.mark();
     u32 *f01 = c.arena.alloc<u32>(n);
     u32 *pos = c.arena.alloc<u32>(n);
@@ -303,12 +500,8 @@ void compact_indices_dn(Ctx &c, const u32 *flags, u32 *out, u64 n, u32 *d_count)
 u32 compact_indices(Ctx &c, const u32 *flags, u32 *out, u64 n) {
     if (n == 0) return 0;
     size_t m = c.arena.mark();
-    u32 *f01 = c.arena.alloc<u32>(n);
-    u32 *pos = c.arena.alloc<u32>(n);
     u32 *tot = c.arena.alloc<u32>(1);
-    LAUNCH(c, k_flag_to_u32, grid_for(c, n), 256, 0, flags, f01, n);
-    scan_excl_u32(c, f01, pos, n);
-    LAUNCH(c, k_compact_write, grid_for(c, n), 256, 0, flags, pos, out, n, tot);
+    compact_indices_dn(c, flags, out, n, tot);
     u32 r = fetch1(c, tot);
     c.arena.release(m);
     return r;

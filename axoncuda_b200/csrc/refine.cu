@@ -176,7 +176,18 @@ struct GainArgs {
     u32 *target;
     i64 *gain;
     u32 *status;
+    const u32 *dyn;  // when set: discount and round read from device memory (graph replays)
 };
+
+// The launch's arguments with the per-round scalars resolved.
+__device__ __forceinline__ GainArgs gain_args_now(const GainArgs &A0) {
+    GainArgs A = A0;
+    if (A0.dyn) {
+        A.discount = A0.dyn[0];
+        A.round = A0.dyn[1];
+    }
+    return A;
+}
 
 __device__ __forceinline__ i64 leave_gain(int encourage, u32 w, u32 c) {
     if (encourage) return c >= 1 ? (i64)((u64)w / ((u64)c * c)) : 0;
@@ -275,8 +286,9 @@ constexpr u32 GN_WARPS = 4;
 constexpr u32 GN_BLOCK = 256;
 constexpr u32 GN_BLOCK_W = 4096;
 
-__global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u32 *__restrict__ list, u32 nl,
+__global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const u32 *__restrict__ list, u32 nl,
                                                              const u64 *__restrict__ work) {
+    const GainArgs A = gain_args_now(A0);
     __shared__ u32 tk[GN_WARPS][2 * GN_WARP_W], td[GN_WARPS][2 * GN_WARP_W];
     __shared__ unsigned long long tcw[GN_WARPS][2 * GN_WARP_W];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -356,8 +368,9 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A, const u
     }
 }
 
-__global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A, const u32 *__restrict__ list, u32 nl, u32 cap_max,
+__global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 *__restrict__ list, u32 nl, u32 cap_max,
                                                         u32 *gtab, const u64 *__restrict__ work) {
+    const GainArgs A = gain_args_now(A0);
     extern __shared__ unsigned long long dyn64[];
     __shared__ i64 red[2][32];
     __shared__ Cand cred[32];
@@ -412,6 +425,13 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A, const u32 *
     }
 }
 
+__global__ void k_list_degree(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ toff,
+                              unsigned long long *__restrict__ out) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 d = i < nl ? toff[list[i] + 1] - toff[list[i]] : 0;
+    d = warp_sum(d);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(out, (unsigned long long)d);
+}
 __global__ void k_tier(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
     // the first tier (lo == 0) also takes nodes without incident hyperedges
@@ -593,10 +613,6 @@ __global__ void k_gather_g2(const u32 *__restrict__ mv, const u32 *__restrict__ 
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nmax) G[i] = i < *dM ? (i64)g2[mv[i]] : 0;
 }
-__global__ void k_incl_fix(const i64 *__restrict__ x, i64 *__restrict__ ex, u32 nmax) {  // ex := ex + x
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nmax) ex[i] += x[i];
-}
 
 // size events: 2r = leave p, 2r+1 = join q
 __global__ void k_size_events(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ part,
@@ -757,6 +773,7 @@ GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp,
     A.off = L.off; A.lam = cs.lam; A.cpart = cs.part; A.ccnt = cs.cnt; A.cdcnt = cs.dcnt; A.wfx = wfx;
     A.toff = L.toff; A.touch = L.touch; A.nin = L.nin; A.nsize = L.nsize; A.part = part;
     A.psize = psize; A.pinb = pinb; A.target = target; A.gain = gain; A.status = status;
+    A.dyn = nullptr;
     return A;
 }
 
@@ -775,6 +792,7 @@ struct LevelPrep {
     u64 gain_bound = 0;      // no gain exceeds this (sum of incident weights)
     u64 max_len = 0;         // largest hyperedge
     u64 dst_pins = 0;        // destination pins (bounds the inbound events: 2 per pin)
+    u64 tier_deg[3] = {0, 0, 0};  // incidence entries of each gain tier (kernel timer only)
 };
 
 void setup_refine_kernels(Ctx &c) {
@@ -815,6 +833,13 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
         }
         lp.gain_bound = fetch1(c, (const u64 *)wm);
         if (lp.ncount[2]) lp.heavy_work_max = reduce_max_u64(c, work, n);
+        if (c.profiling("k_gain_warp") || c.profiling("k_gain_block")) {
+            unsigned long long *dg = c.arena.alloc<unsigned long long>(3);
+            AXC_CUDA(cudaMemsetAsync(dg, 0, 24, c.stream));
+            for (int t = 0; t < 3; ++t)
+                LAUNCH(c, k_list_degree, cdiv(lp.ncount[t], 256), 256, 0, lp.ntier[t], lp.ncount[t], L.toff, dg + t);
+            fetch(c, lp.tier_deg, dg, 24);
+        }
     }
     return lp;
 }
@@ -845,8 +870,15 @@ static Census alloc_census(Ctx &c, const DLevel &L) {
     return cs;
 }
 
+// Algorithmic bytes of one gains launch over a node list: 8 per incidence entry (the touching id
+// and the census reads of the node's own and the candidate partitions) and 16 per node (its
+// move, gain and rank).
+static u64 gain_bytes(const LevelPrep &lp, int t) { return 8 * lp.tier_deg[t] + 16 * (u64)lp.ncount[t]; }
+
 static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainArgs &A) {
     fill_u32(c, A.target, NONE, L.n);
+    if (c.profiling("k_gain_warp") && lp.ncount[0]) c.prof_bytes += gain_bytes(lp, 0);
+    if (c.profiling("k_gain_block")) c.prof_bytes += gain_bytes(lp, 1) + gain_bytes(lp, 2);
     LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
     LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, 2 * GN_BLOCK_W * 16, A, lp.ntier[1], lp.ncount[1], 2 * GN_BLOCK_W,
            (u32 *)nullptr, lp.work);
@@ -911,11 +943,15 @@ void refine_gains_only(Ctx &c, const DLevel &L, const u32 *wfx, const RefinePara
     c.arena.release(m);
 }
 
-// One round; returns true when moves were applied. One host round trip (the apply flag).
-static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
-                         u32 *part, u32 discount, u32 round) {
+// The launches of one round, with no host synchronization: safe to capture in a CUDA graph.
+// dyn (device, optional) holds the round's discount and round number for graph replays. Returns
+// the device word that says whether the moves were applied; its arena slot lies below `keep`,
+// the mark the caller releases to after reading it.
+static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
+                       u32 *part, u32 discount, u32 round, const u32 *dyn, size_t &keep) {
     const u32 n = L.n;
-    size_t m0 = c.arena.mark();
+    u32 *apply = c.arena.alloc<u32>(1);
+    keep = c.arena.mark();
     Census cs = alloc_census(c, L);
     run_census(c, L, lp, part, cs);
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
@@ -924,6 +960,7 @@ static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32
     u32 *target = c.arena.alloc<u32>(n);
     i64 *gain = c.arena.alloc<i64>(n);
     GainArgs A = make_gain_args(L, wfx, rp, cs, part, psize, pinb, discount, round, target, gain, c.d_status);
+    A.dyn = dyn;
     run_gains(c, L, lp, A);
     // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
     // [3] big cascade hyperedges
@@ -986,8 +1023,7 @@ static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32
     // prefix gains in rank order
     i64 *G = c.arena.alloc<i64>(n), *Gx = c.arena.alloc<i64>(n);
     LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);
-    scan_excl_i64(c, Gx, G, n);
-    LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Gx, G, n);
+    scan_incl_i64(c, Gx, G, n);
     // size validity
     i64 *Vs = c.arena.alloc<i64>(n);
     AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)n * 8, c.stream));
@@ -1006,8 +1042,7 @@ static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32
         c.arena.release(m1);
     }
     i64 *Vsx = c.arena.alloc<i64>(n);
-    scan_excl_i64(c, Vs, Vsx, n);
-    LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Vs, Vsx, n);
+    scan_incl_i64(c, Vs, Vsx, n);
     Vs = Vsx;
     // inbound validity (INCC only): the transitions ordered by (partition, rank), the running
     // inbound-set size of each partition along them
@@ -1041,18 +1076,21 @@ static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32
                (unsigned long long *)Vi);
         c.arena.release(m1);
         i64 *Vix = c.arena.alloc<i64>(n);
-        scan_excl_i64(c, Vi, Vix, n);
-        LAUNCH(c, k_incl_fix, cdiv(n, 256), 256, 0, Vi, Vix, n);
+        scan_incl_i64(c, Vi, Vix, n);
         Vi = Vix;
     }
     // best prefix and apply
     const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
     Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
-    u32 *apply = c.arena.alloc<u32>(1);
     LAUNCH(c, k_best, nbk, 256, 0, G, Vs, Vi, dM, bb + 1);
     LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, Vi, bb, apply);
     LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
-    // one round trip: the apply flag and the status word
+    c.arena.release(keep);
+    return apply;
+}
+
+// The round's one host round trip: the apply flag and the status word.
+static bool round_result(Ctx &c, const u32 *apply) {
     AXC_CUDA(cudaMemcpyAsync(c.h_pinned, apply, 4, cudaMemcpyDeviceToHost, c.stream));
     AXC_CUDA(cudaMemcpyAsync((char *)c.h_pinned + 4, c.d_status, 4, cudaMemcpyDeviceToHost, c.stream));
     AXC_CUDA(cudaStreamSynchronize(c.stream));
@@ -1062,8 +1100,42 @@ static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32
         AXC_CUDA(cudaMemsetAsync(c.d_status, 0, 4, c.stream));
         throw Error(AXC_EINTERNAL, "device status word = " + std::to_string(hv[1]));
     }
-    c.arena.release(m0);
     return hv[0] != 0;
+}
+
+// One round, launched eagerly; returns true when moves were applied.
+static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
+                         u32 *part, u32 discount, u32 round) {
+    const size_t m0 = c.arena.mark();
+    size_t keep;
+    const u32 *apply = round_body(c, L, lp, wfx, rp, part, discount, round, nullptr, keep);
+    const bool r = round_result(c, apply);
+    c.arena.release(m0);
+    return r;
+}
+
+// The rounds of one level replayed from one CUDA graph of the round body.
+struct RoundGraph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    ~RoundGraph() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+// Kernel nodes of a captured graph (memset and copy nodes are not kernel launches).
+static u32 rg_kernels(cudaGraph_t g) {
+    size_t k = 0;
+    if (cudaGraphGetNodes(g, nullptr, &k) != cudaSuccess || k == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(k);
+    if (cudaGraphGetNodes(g, nodes.data(), &k) != cudaSuccess) return 0;
+    u32 kernels = 0;
+    for (size_t i = 0; i < k; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    return kernels;
 }
 
 // level bounds that need the offsets: the largest hyperedge and the destination pin count
@@ -1097,16 +1169,67 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
         lp.max_len = h[0];
         lp.dst_pins = h[1];
     }
+    // Graph replays need the round's scalars in device memory. Kernel-timer pairs captured in the
+    // graph are read back after every replay; the bytes of the captured launches count per replay.
+    const bool graph = R > 1;
+    size_t ev0 = 0, ev1 = 0;
+    u64 bytes_per_round = 0;
+    RoundGraph rg;
+    u32 *dyn = nullptr, *apply = nullptr, graph_kernels = 0;
+    if (graph) {
+        dyn = c.arena.alloc<u32>(2);
+        const size_t m1 = c.arena.mark();
+        size_t keep;
+        const u32 launches0 = c.launches;  // captured launches run only when replayed
+        const u64 bytes0 = c.prof_bytes;
+        ev0 = c.prof_used;
+        AXC_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        c.capturing = true;
+        try {
+            apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep);
+        } catch (...) {
+            c.capturing = false;
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(c.stream, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        c.capturing = false;
+        ev1 = c.prof_used;
+        bytes_per_round = c.prof_bytes - bytes0;
+        c.prof_bytes = bytes0;
+        AXC_CUDA(cudaStreamEndCapture(c.stream, &rg.g));
+        AXC_CUDA(cudaGraphInstantiate(&rg.x, rg.g, 0));
+        c.launches = launches0;
+        graph_kernels = rg_kernels(rg.g);
+        c.arena.release(m1);
+        c.arena.alloc<u32>(1);  // keep the apply word below the round's scratch, as captured
+    }
     u32 done = 0;
     for (u32 r = 0; r < R; ++r) {
         const u32 discount = r < R / 3 ? 1u : (r < 2 * R / 3 ? 2u : 0xFFFFFFFFu);
         ++done;
-        if (!refine_round(c, L, lp, wfx, rp, part, discount, r)) {
+        bool applied;
+        if (graph) {
+            u32 *hp = (u32 *)((char *)c.h_pinned + 64);
+            hp[0] = discount;
+            hp[1] = r;
+            AXC_CUDA(cudaMemcpyAsync(dyn, hp, 8, cudaMemcpyHostToDevice, c.stream));
+            AXC_CUDA(cudaGraphLaunch(rg.x, c.stream));
+            c.launches += graph_kernels;
+            applied = round_result(c, apply);
+            c.prof_collect(ev0, ev1);
+            c.prof_bytes += bytes_per_round;
+        } else {
+            applied = refine_round(c, L, lp, wfx, rp, part, discount, r);
+        }
+        if (!applied) {
             if (r < R / 3) r = R / 2;
             else if (r < 2 * R / 3) r = 2 * R / 3;
             else r = R;
         }
     }
+    if (graph) c.prof_used = ev0;  // the captured pairs go back to the pool with the graph
     c.arena.release(m);
     return done;
 }

@@ -129,13 +129,30 @@ def barrier(world):
         dist.barrier()
 
 
-def traffic_model(st) -> dict:
-    """Algorithmic bytes of the rating kernel per step (each node streams its incident hyperedges'
-    pins: 4 B per pin visit, plus 28 B per incidence entry for the touching list, offsets, weight
-    and source count)."""
-    visits = int(st.rating_pin_visits)
-    touch = sum(int(st.level_pins[i]) for i in range(min(int(st.levels), 64)))
-    return {"rating_bytes": 4 * visits + 28 * touch, "pin_visits": visits}
+ROOFLINE_KERNEL = "k_gain_warp"  # the kernel with the largest share of device time (profiles/)
+
+
+def hbm_peak() -> tuple[float, str]:
+    """Measured copy bandwidth of this pool's B200s (GB/s), else the stated fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of the kernel from its committed ncu summary, if there is one."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}-{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9]+)", line)
+                if m:
+                    return int(m.group(1))
+    except OSError:
+        pass
+    return None
 
 
 def run_ours(args, world, rank, local):
@@ -171,7 +188,11 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     total_ms = 0.0
     launches = 0
-    rating_ms = []
+    # the dominant kernel is timed with events on the library's own stream, launch by launch
+    kname = args.roofline_kernel
+    ctx.profile_kernel(kname)
+    ctx.profile_read()
+    k_launches, k_ms, k_bytes = 0, 0.0, 0
     with Clocks(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -184,6 +205,11 @@ def run_ours(args, world, rank, local):
             torch.cuda.synchronize()
             total_ms += e0.elapsed_time(e1)
             launches += int(st.kernel_launches)
+            kt = ctx.profile_read()
+            k_launches += kt.launches
+            k_ms += kt.ms_total
+            k_bytes += kt.bytes
+    ctx.profile_kernel(None)
     total_ms = barrier_max(world, total_ms)
     ms_step = total_ms / args.steps
     value = world * P / (ms_step / 1e3)
@@ -233,9 +259,19 @@ def run_ours(args, world, rank, local):
                     "valid": int(st2.valid), "levels": int(st2.levels)},
         "clocks": clk.summary(),
     }
-    tm = traffic_model(st)
-    out["roofline"] = None
-    out["_traffic_model"] = tm
+    peak, peak_kind = hbm_peak()
+    achieved = (k_bytes / (k_ms / 1e3)) / 1e9 if k_ms > 0 else 0.0
+    traffic = profiled_traffic(kname, args.workload)
+    out["roofline"] = {
+        "bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak if peak else None, "peak_source": peak_kind,
+        "traffic": traffic,
+        "bytes_per_launch": k_bytes / k_launches if k_launches else 0,
+        "ms_per_launch": k_ms / k_launches if k_launches else 0,
+        "launches_per_step": k_launches / args.steps,
+        "share_of_step": (k_ms / args.steps) / ms_step if ms_step else None,
+        "model": "8 B per incidence entry of the listed nodes + 16 B per listed node",
+    }
     ctx.close()
     return out, g, p, part
 
@@ -309,6 +345,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--roofline-kernel", default=ROOFLINE_KERNEL)
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -114,6 +114,20 @@ void axc_destroy(axc_ctx *ctx);
 const char *axc_strerror(int status);
 const char *axc_last_error(axc_ctx *ctx);   /* human-readable detail of the last failure */
 
+/* ---- kernel timer (measurement; no reference counterpart: the reference times whole phases
+ * with host clocks, sources/main.cu:151-910) ------------------------------------------------------
+ * While a kernel name is set, every launch of that kernel on the context stream is bracketed by a
+ * pair of CUDA events, and launch sites with a byte model add the launch's algorithmic bytes.
+ * axc_profile_read synchronizes the stream, returns the totals since the kernel was set and
+ * resets them. kernel = NULL switches the timer off. */
+typedef struct {
+    uint32_t launches;  /* launches of the kernel seen */
+    double ms_total;    /* sum of their event-timed durations */
+    uint64_t bytes;     /* sum of their algorithmic bytes (0 if the kernel has no byte model) */
+} axc_kernel_timing;
+int axc_profile_kernel(axc_ctx *ctx, const char *kernel);
+int axc_profile_read(axc_ctx *ctx, axc_kernel_timing *out);
+
 /* Defaults of sources/runconfig.cpp:48-70 (cnc=16, rfr=16, smh=2, om=1.5) with the given mode. */
 void axc_params_default(axc_params *p, int mode);
 /* Preset constraints of sources/constr.cpp:195-229: "loihi64", "loihi84", "loihi1024", "truenorth". */
