@@ -77,7 +77,7 @@ EXPORTS = [
     "axc_write_hgraph", "axc_write_partition", "axc_read_partition", "axc_quotient_hgraph",
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
-    "axc_stage_gains", "axc_profile_kernel", "axc_profile_read",
+    "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
 ]
 
 _lib = None
@@ -129,6 +129,8 @@ def lib() -> C.CDLL:
         }
         sig["axc_profile_kernel"] = (C.c_int, [C.c_void_p, C.c_char_p])
         sig["axc_profile_read"] = (C.c_int, [C.c_void_p, C.POINTER(KernelTiming)])
+        sig["axc_connectivity_noalloc"] = (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                     C.c_void_p, C.POINTER(C.c_int64)])
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res

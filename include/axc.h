@@ -245,6 +245,27 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
                     const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage,
                     uint32_t discount, uint32_t *out_target, int64_t *out_gain);
 
+/* ---- connectivity without allocating (no reference counterpart) ---------------------------------
+ * out_fx[0..2] = connectivity_fx, cutnet_fx and soed_fx of part[] over a hypergraph already in
+ * device memory, equal to what axc_evaluate reports for the same inputs. For callers that may not
+ * allocate device memory: a serving loop whose memory is all committed to resident hierarchies
+ * under its admission budget, or a host runtime whose pool allocator owns the device and leaves no
+ * room for the arena an axc_ctx reserves. It needs no context and calls no allocating routine: its
+ * scratch is one fixed 16 MiB array in the library's device image, and it clears the part of that
+ * array that must start at zero on every call.
+ * - Runs on the current device, on `stream` (a cudaStream_t; NULL = the default stream), and
+ *   synchronizes that stream before returning.
+ * - The first call on each device looks up the scratch address; make that call before any stream
+ *   capture.
+ * - Hyperedges longer than 16384 pins are refused with AXC_EOVERFLOW; a partition id of
+ *   UINT32_MAX gives AXC_EINVAL.
+ * - Calls that overlap on the GPU (other streams, other host threads) share the scratch and race:
+ *   serialize them on one device.
+ * d_hedge_off[e+1], d_pins, d_part[n]: device memory; d_hedge_w may be NULL (unit weights). */
+int axc_connectivity_noalloc(uint32_t e, const uint64_t *d_hedge_off, const uint32_t *d_pins,
+                             const float *d_hedge_w, const uint32_t *d_part, void *stream,
+                             int64_t *out_fx);
+
 #ifdef __cplusplus
 }
 #endif
