@@ -61,6 +61,7 @@ class Stats(C.Structure):
         ("ms_device", C.c_double), ("ms_core", C.c_double), ("kernel_launches", C.c_uint32),
         ("level_pins", C.c_uint64 * 64), ("level_nodes", C.c_uint32 * 64),
         ("refine_rounds", C.c_uint32 * 64), ("rating_pin_visits", C.c_uint64),
+        ("device_bytes_peak", C.c_uint64), ("ms_queued", C.c_double), ("ms_run", C.c_double),
     ]
 
 
@@ -78,6 +79,7 @@ EXPORTS = [
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
     "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
+    "axc_serve_configure",
 ]
 
 _lib = None
@@ -131,6 +133,8 @@ def lib() -> C.CDLL:
         sig["axc_profile_read"] = (C.c_int, [C.c_void_p, C.POINTER(KernelTiming)])
         sig["axc_connectivity_noalloc"] = (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                      C.c_void_p, C.POINTER(C.c_int64)])
+        sig["axc_serve_configure"] = (C.c_int, [C.c_void_p, C.c_uint32, C.c_size_t])
+        sig["axc_partition_batch"] = (C.c_int, [C.c_void_p, C.c_uint32, H, P, C.POINTER(u32p), S])
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res
@@ -303,6 +307,21 @@ class Context:
         st = Stats()
         self._check(lib().axc_poll(self._h, jid, _ptr(out, C.c_uint32), C.byref(st), timeout_ms), "axc_poll")
         return out[:n], st
+
+    def serve_configure(self, lanes: int, device_budget: int = 0):
+        """Lanes and device-memory budget of the batching / serving executor (before any submit)."""
+        self._check(lib().axc_serve_configure(self._h, lanes, device_budget), "axc_serve_configure")
+
+    def partition_batch(self, jobs: list[tuple[Hypergraph, Params]]) -> list[tuple[np.ndarray, Stats]]:
+        """All jobs through the executor's lanes in one call (axc_partition_batch)."""
+        k = len(jobs)
+        hg = (HGraph * k)(*[g.c() for g, _ in jobs])
+        ps = (Params * k)(*[p for _, p in jobs])
+        outs = [np.zeros(max(g.n, 1), np.uint32) for g, _ in jobs]
+        ptrs = (C.POINTER(C.c_uint32) * k)(*[_ptr(o, C.c_uint32) for o in outs])
+        sts = (Stats * k)()
+        self._check(lib().axc_partition_batch(self._h, k, hg, ps, ptrs, sts), "axc_partition_batch")
+        return [(outs[i][: jobs[i][0].n], sts[i]) for i in range(k)]
 
     # ---- stages (host buffers in/out) ----
     def stage_construct(self, g: Hypergraph):

@@ -1,6 +1,7 @@
 // Host-only helpers shared by the readers, writers, generators and the driver.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/axc.h"
@@ -17,6 +18,16 @@ struct HostGraph {
 };
 
 void publish(HostGraph *hg, axc_hgraph *out);
+
+// Lanes of the batching / serving executor (driver.cu): a stream, status word and scan state of
+// their own; each job runs in a fresh device arena of the size the executor grants it.
+struct Lane;
+int ctx_device(axc_ctx *ctx);
+size_t device_free_bytes(int device);
+Lane *lane_create(int device, int *rc);
+void lane_destroy(Lane *l);
+int lane_partition(Lane *l, size_t arena_bytes, const axc_hgraph *g, const axc_params *p, uint32_t *out_part,
+                   axc_stats *stats, std::string *err);
 
 // splitmix64: seeds independent xoshiro streams per (seed, index) so generators are
 // deterministic under any thread count.

@@ -1,6 +1,10 @@
-// Job queue behind axc_submit / axc_poll / axc_partition_batch: a worker thread owns the device
-// context and runs admitted jobs; callers wait on per-job completion. Admission compares a job's
-// device-memory estimate against the context arena.
+// Batching and serving behind axc_serve_configure / axc_submit / axc_poll / axc_partition_batch:
+// continuous batching over a pool of lanes. Each lane is a worker thread with its own stream; a
+// job runs on one lane in a device arena of its estimated size. Jobs start in submission order
+// as lanes and device memory free up, with smaller jobs allowed past one that does not fit yet,
+// so independent jobs overlap on the device.
+#include <algorithm>
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -13,9 +17,10 @@
 #include "axc_host.h"
 
 struct axc_ctx;
-extern "C" int axc_partition(axc_ctx *, const axc_hgraph *, const axc_params *, uint32_t *, axc_stats *);
 
 namespace axc {
+
+using Clock = std::chrono::steady_clock;
 
 struct Job {
     uint64_t id = 0;
@@ -24,54 +29,135 @@ struct Job {
     axc_params p{};
     std::vector<uint32_t> part;
     axc_stats st{};
+    size_t est = 0;  // device bytes granted
+    int retries = 0;
     int rc = 0;
     bool done = false;
+    std::string err;
+    Clock::time_point t_submit, t_start, t_end;
 };
 
-struct BatchState {
-    axc_ctx *ctx = nullptr;
-    std::thread worker;
+// Device bytes a job's arena needs: the level hierarchy, one refinement round's scratch (the
+// inbound transitions, at most two per destination pin, dominate it) and the sorts' buffers.
+// A job that runs out is retried once with twice as much.
+static size_t estimate_bytes(const axc_hgraph *g) {
+    const uint64_t P = g->e ? g->hedge_off[g->e] : 0;
+    const double b = 192.0 * (double)P + 160.0 * (double)g->n + 96.0 * (double)g->e + (64u << 20);
+    return (size_t)b;
+}
+
+struct Executor {
+    int device = 0;
+    uint32_t nlanes = 1;
+    size_t budget = 0;
+    std::vector<Lane *> lanes;
+    std::vector<std::thread> threads;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Job *> queue;
     std::map<uint64_t, std::unique_ptr<Job>> jobs;
+    size_t in_use = 0;
+    uint32_t running = 0;
     bool stop = false;
     uint64_t next_id = 1;
 
-    void run() {
+    // The first queued job that fits next to the running ones; with nothing running, the head.
+    Job *pick() {
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+            if (running == 0 || (*it)->est <= budget - std::min(budget, in_use)) {
+                Job *j = *it;
+                queue.erase(it);
+                return j;
+            }
+        }
+        return nullptr;
+    }
+
+    void run(uint32_t li) {
+        Lane *lane = lanes[li];
         for (;;) {
             Job *j = nullptr;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-                if (stop && queue.empty()) return;
-                j = queue.front();
-                queue.pop_front();
+                cv_work.wait(lk, [&] { return stop || (!queue.empty() && (j = pick()) != nullptr); });
+                if (!j) return;  // stopping
+                in_use += j->est;
+                ++running;
             }
-            int rc = axc_partition(ctx, &j->view, &j->p, j->part.data(), &j->st);
+            j->t_start = Clock::now();
+            std::string err;
+            const int rc = lane_partition(lane, j->est, &j->view, &j->p, j->part.data(), &j->st, &err);
+            j->t_end = Clock::now();
+            bool requeued = false;
             {
                 std::lock_guard<std::mutex> lk(mu);
-                j->rc = rc;
-                j->done = true;
+                in_use -= j->est;
+                --running;
+                if (rc == AXC_ENOMEM && j->retries == 0) {
+                    j->retries = 1;
+                    j->est *= 2;
+                    queue.push_front(j);
+                    requeued = true;
+                } else {
+                    j->rc = rc;
+                    j->err = err;
+                    j->st.ms_queued = std::chrono::duration<double, std::milli>(j->t_start - j->t_submit).count();
+                    j->st.ms_run = std::chrono::duration<double, std::milli>(j->t_end - j->t_start).count();
+                    j->done = true;
+                }
             }
-            cv_done.notify_all();
+            cv_work.notify_all();
+            if (!requeued) cv_done.notify_all();
         }
+    }
+
+    int start(int dev) {
+        device = dev;
+        for (uint32_t i = 0; i < nlanes; ++i) {
+            int rc = AXC_OK;
+            Lane *l = lane_create(device, &rc);
+            if (!l) return rc;
+            lanes.push_back(l);
+        }
+        for (uint32_t i = 0; i < nlanes; ++i) threads.emplace_back([this, i] { run(i); });
+        return AXC_OK;
+    }
+
+    ~Executor() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv_work.notify_all();
+        for (auto &t : threads)
+            if (t.joinable()) t.join();
+        for (Lane *l : lanes) lane_destroy(l);
     }
 };
 
-// per-context batching state, created lazily
+// per-context executor, created at the first submit with the configured lanes and budget
 static std::mutex g_mu;
-static std::map<axc_ctx *, std::unique_ptr<BatchState>> g_states;
+static std::map<axc_ctx *, std::unique_ptr<Executor>> g_exec;
+static std::map<axc_ctx *, std::pair<uint32_t, size_t>> g_config;
 
-static BatchState *state_for(axc_ctx *ctx) {
+static Executor *executor_for(axc_ctx *ctx, int *rc) {
     std::lock_guard<std::mutex> lk(g_mu);
-    auto &s = g_states[ctx];
-    if (!s) {
-        s.reset(new BatchState());
-        s->ctx = ctx;
-        s->worker = std::thread([p = s.get()] { p->run(); });
+    auto it = g_exec.find(ctx);
+    if (it != g_exec.end()) {
+        *rc = AXC_OK;
+        return it->second.get();
     }
-    return s.get();
+    auto x = std::make_unique<Executor>();
+    auto cfg = g_config.find(ctx);
+    x->nlanes = cfg != g_config.end() ? cfg->second.first : 1;
+    size_t budget = cfg != g_config.end() ? cfg->second.second : 0;
+    if (budget == 0) budget = device_free_bytes(ctx_device(ctx)) / 2;
+    x->budget = budget;
+    *rc = x->start(ctx_device(ctx));
+    if (*rc) return nullptr;
+    Executor *p = x.get();
+    g_exec[ctx] = std::move(x);
+    return p;
 }
 
 }  // namespace axc
@@ -79,29 +165,36 @@ static BatchState *state_for(axc_ctx *ctx) {
 using namespace axc;
 
 extern "C" void axc_batch_free(axc_ctx *ctx) {
-    std::unique_ptr<BatchState> s;
+    std::unique_ptr<Executor> e;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        auto it = g_states.find(ctx);
-        if (it == g_states.end()) return;
-        s = std::move(it->second);
-        g_states.erase(it);
+        g_config.erase(ctx);
+        auto it = g_exec.find(ctx);
+        if (it == g_exec.end()) return;
+        e = std::move(it->second);
+        g_exec.erase(it);
     }
-    {
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->stop = true;
-    }
-    s->cv_work.notify_all();
-    if (s->worker.joinable()) s->worker.join();
+    e.reset();  // joins the lane threads
+}
+
+extern "C" int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_budget) {
+    if (!ctx || lanes == 0 || lanes > 256) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_exec.count(ctx)) return AXC_EBUSY;  // already serving
+    g_config[ctx] = {lanes, device_budget};
+    return AXC_OK;
 }
 
 extern "C" int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint64_t *job_id) {
     if (!ctx || !g || !p || !job_id) return AXC_EINVAL;
-    auto j = std::make_unique<Job>();
+    if (g->e && (!g->hedge_off || !g->src_count)) return AXC_EINVAL;
     const uint64_t P = g->e ? g->hedge_off[g->e] : 0;
+    if (P && !g->pins) return AXC_EINVAL;
+    auto j = std::make_unique<Job>();
+    j->t_submit = Clock::now();
     j->g.n = g->n;
-    j->g.off.assign(g->hedge_off, g->hedge_off + g->e + 1);
-    if (!g->e) j->g.off.assign(1, 0);
+    if (g->e) j->g.off.assign(g->hedge_off, g->hedge_off + g->e + 1);
+    else j->g.off.assign(1, 0);
     j->g.pins.assign(g->pins, g->pins + P);
     j->g.nsrc.assign(g->src_count, g->src_count + g->e);
     if (g->hedge_w) j->g.w.assign(g->hedge_w, g->hedge_w + g->e);
@@ -114,41 +207,56 @@ extern "C" int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p
     j->view.hedge_w = j->g.w.data();
     j->p = *p;
     j->part.assign(g->n ? g->n : 1, 0);
-    BatchState *s = state_for(ctx);
+    j->est = estimate_bytes(g);
+    int rc = AXC_OK;
+    Executor *x = executor_for(ctx, &rc);
+    if (!x) return rc;
     {
-        std::lock_guard<std::mutex> lk(s->mu);
-        j->id = s->next_id++;
+        std::lock_guard<std::mutex> lk(x->mu);
+        j->id = x->next_id++;
         *job_id = j->id;
-        s->queue.push_back(j.get());
-        s->jobs[j->id] = std::move(j);
+        x->queue.push_back(j.get());
+        x->jobs[j->id] = std::move(j);
     }
-    s->cv_work.notify_one();
+    x->cv_work.notify_all();
     return AXC_OK;
 }
 
 extern "C" int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms) {
     if (!ctx) return AXC_EINVAL;
-    BatchState *s = state_for(ctx);
-    std::unique_lock<std::mutex> lk(s->mu);
-    auto it = s->jobs.find(job_id);
-    if (it == s->jobs.end()) return AXC_ENOTFOUND;
+    int rc = AXC_OK;
+    Executor *x = executor_for(ctx, &rc);
+    if (!x) return rc;
+    std::unique_lock<std::mutex> lk(x->mu);
+    auto it = x->jobs.find(job_id);
+    if (it == x->jobs.end()) return AXC_ENOTFOUND;
     Job *j = it->second.get();
     auto ready = [&] { return j->done; };
-    if (timeout_ms < 0) s->cv_done.wait(lk, ready);
-    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return AXC_ETIMEDOUT;
-    int rc = j->rc;
+    if (timeout_ms < 0) x->cv_done.wait(lk, ready);
+    else if (!x->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return AXC_ETIMEDOUT;
+    rc = j->rc;
     if (out_part && j->g.n) std::memcpy(out_part, j->part.data(), (size_t)j->g.n * 4);
     if (stats) *stats = j->st;
-    s->jobs.erase(it);
+    x->jobs.erase(it);
     return rc;
 }
 
 extern "C" int axc_partition_batch(axc_ctx *ctx, uint32_t count, const axc_hgraph *g, const axc_params *p,
                                    uint32_t *const *out_parts, axc_stats *stats) {
     if (!ctx || (count && (!g || !p || !out_parts))) return AXC_EINVAL;
+    std::vector<uint64_t> ids(count, 0);
+    int first = AXC_OK;
     for (uint32_t i = 0; i < count; ++i) {
-        int rc = axc_partition(ctx, &g[i], &p[i], out_parts[i], stats ? &stats[i] : nullptr);
-        if (rc) return rc;
+        const int rc = axc_submit(ctx, &g[i], &p[i], &ids[i]);
+        if (rc) {
+            ids[i] = 0;
+            if (!first) first = rc;
+        }
     }
-    return AXC_OK;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!ids[i]) continue;
+        const int rc = axc_poll(ctx, ids[i], out_parts[i], stats ? &stats[i] : nullptr, -1);
+        if (rc && !first) first = rc;
+    }
+    return first;
 }

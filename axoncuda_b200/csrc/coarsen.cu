@@ -18,6 +18,9 @@ namespace cg = cooperative_groups;
 namespace axc {
 namespace {
 
+// Pins a hyperedge contributes to the rating: all of them up to AXC_RATE_MAX_LEN, none above.
+__host__ __device__ __forceinline__ u32 rated_len(u64 len) { return len <= AXC_RATE_MAX_LEN ? (u32)len : 0u; }
+
 constexpr u32 RT_WARP_W = 256;     // work (incident pins) handled by one warp
 constexpr u32 RT_BLK1_W = 2048;    // block tier 1: table 4096 slots (48 KiB)
 constexpr u32 RT_BLK2_W = 8192;    // block tier 2: table 16384 slots (192 KiB)
@@ -31,7 +34,7 @@ __global__ void k_rate_work(u32 n, const u64 *__restrict__ toff, const u32 *__re
     u64 s = 0;
     for (u64 j = toff[u] + lane; j < toff[u + 1]; j += 32) {
         u32 h = touch[j];
-        s += off[h + 1] - off[h];
+        s += rated_len(off[h + 1] - off[h]);
     }
     s = warp_sum(s);
     if (lane == 0) work[u] = s;
@@ -53,96 +56,54 @@ struct RateArgs {
     u32 *status;
 };
 
-// Accumulate node u's neighbour scores into (keys, sc, cm) of size mask+1, using `nt` threads with
-// index t; `scratch` holds per-thread chunk info for the block variant (nullptr: warp variant).
-template <bool WARP>
-__device__ void rate_accumulate(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 t,
-                                u32 nt, u32 *sh_excl, u32 *sh_a, u32 *sh_c, u32 *sh_s, u32 *sh_inb,
-                                u32 *sh_tot) {
-    const u64 t0 = A.toff[u], t1 = A.toff[u + 1];
-    const u32 deg = (u32)(t1 - t0), nin_u = A.nin[u];
-    for (u32 jb = 0; jb < deg; jb += nt) {
-        const u32 j = jb + t;
+// Accumulate node u's neighbour scores into (keys, sc, cm) of size mask+1. Warp-cooperative: the
+// calling warp takes u's incidences in batches of 32 starting at `first`, every `stride` entries.
+// A batch's hyperedge metadata loads in parallel, then its pins are flattened across the lanes
+// (each lane finds its pin's hyperedge by a 5-step search over the prefix of the batch's lengths).
+__device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 first,
+                          u32 stride) {
+    const u32 lane = threadIdx.x & 31u;
+    const u64 t0 = A.toff[u];
+    const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
+    for (u32 jb = first; jb < deg; jb += stride) {
+        const u32 j = jb + lane;
         const bool has = j < deg;
-        u32 h = has ? A.touch[t0 + j] : 0;
-        u64 a = has ? A.off[h] : 0;
-        u32 len = has ? (u32)(A.off[h + 1] - a) : 0;
-        u32 c = has ? A.wfx[h] / len : 0;
-        u32 s_end = has ? (u32)A.nsrc[h] : 0;  // sources occupy [0, s_end)
-        u32 inb = (has && j < nin_u) ? 1u : 0u;
-        u32 excl, total;
-        if (WARP) {
-            u32 x = len;
+        const u32 h = has ? A.touch[t0 + j] : 0;
+        const u64 a = has ? A.off[h] : 0;
+        const u32 len = has ? rated_len(A.off[h + 1] - a) : 0;  // 0: not rated
+        const u32 c = len ? A.wfx[h] / len : 0;
+        const u32 s_end = has ? (u32)A.nsrc[h] : 0;  // sources occupy [0, s_end)
+        const u32 inb = (has && j < nin_u) ? 1u : 0u;
+        u32 x = len;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if ((int)t >= o) x += y;
-            }
-            total = __shfl_sync(0xFFFFFFFFu, x, 31);
-            excl = x - len;
-        } else {
-            // block-wide exclusive scan of len
-            sh_excl[t] = len;
-            __syncthreads();
-            for (u32 o = 1; o < nt; o <<= 1) {
-                u32 y = t >= o ? sh_excl[t - o] : 0;
-                __syncthreads();
-                sh_excl[t] += y;
-                __syncthreads();
-            }
-            excl = sh_excl[t] - len;
-            if (t == nt - 1) *sh_tot = sh_excl[t];
-            __syncthreads();
-            total = *sh_tot;
-            sh_excl[t] = excl;
-            sh_c[t] = c;
-            sh_s[t] = s_end;
-            sh_inb[t] = inb;
-            __syncthreads();
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if ((int)lane >= o) x += y;
         }
-        const u32 chunk = (deg - jb) < nt ? (deg - jb) : nt;
-        for (u32 fb = 0; fb < total; fb += nt) {
-            const u32 f = fb + t;
-            const bool ok = f < total;
-            // owner: largest o < chunk with excl_o <= f
-            u32 lo = 0, hi = chunk - 1;
-            if (WARP) {
-                for (int it = 0; it < 5; ++it) {
-                    const u32 mid = (lo + hi + 1) >> 1;
-                    const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
-                    if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
-                }
-            } else {
-                while (lo < hi) {
-                    u32 mid = (lo + hi + 1) >> 1;
-                    if (sh_excl[mid] <= f) lo = mid; else hi = mid - 1;
-                }
+        const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - len;
+        const u32 chunk = (deg - jb) < 32 ? (deg - jb) : 32;
+        for (u32 fb = 0; fb < total; fb += 32) {
+            const u32 f = fb + lane;
+            u32 lo = 0, hi = chunk - 1;  // owner: largest o < chunk with excl_o <= f
+            for (int it = 0; it < 5; ++it) {
+                const u32 mid = (lo + hi + 1) >> 1;
+                const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
+                if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
             }
-            const u32 o = lo;
-            u32 hh, cc, ss, ib, eo;
-            if (WARP) {
-                hh = __shfl_sync(0xFFFFFFFFu, h, o);
-                cc = __shfl_sync(0xFFFFFFFFu, c, o);
-                ss = __shfl_sync(0xFFFFFFFFu, s_end, o);
-                ib = __shfl_sync(0xFFFFFFFFu, inb, o);
-                eo = __shfl_sync(0xFFFFFFFFu, excl, o);
-            } else {
-                hh = A.touch[t0 + jb + o];
-                cc = sh_c[o];
-                ss = sh_s[o];
-                ib = sh_inb[o];
-                eo = sh_excl[o];
-            }
-            if (!ok) continue;
-            const u32 i = f - eo;  // position inside hyperedge hh
-            const u32 v = A.pins[A.off[hh] + i];
+            const u64 ao = __shfl_sync(0xFFFFFFFFu, a, lo);
+            const u32 cc = __shfl_sync(0xFFFFFFFFu, c, lo);
+            const u32 ss = __shfl_sync(0xFFFFFFFFu, s_end, lo);
+            const u32 ib = __shfl_sync(0xFFFFFFFFu, inb, lo);
+            const u32 eo = __shfl_sync(0xFFFFFFFFu, excl, lo);
+            if (f >= total) continue;
+            const u32 i = f - eo;  // position inside the owner hyperedge
+            const u32 v = A.pins[ao + i];
             if (v == u) continue;
             const u32 slot = hash_find_or_insert(keys, mask, v);
             if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
             atomicAdd(&sc[slot], cc);
             if (ib && i >= ss) atomicAdd(&cm[slot], 1u);
         }
-        if (!WARP) __syncthreads();
     }
 }
 
@@ -164,15 +125,14 @@ __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u
     u32 W = 0;  // work bound for the table size
     for (u64 j = A.toff[u] + lane; j < A.toff[u + 1]; j += 32) {
         u32 h = A.touch[j];
-        W += (u32)(A.off[h + 1] - A.off[h]);
+        W += rated_len(A.off[h + 1] - A.off[h]);
     }
     W = warp_sum(W);
     u32 cap = 64;
     while (cap < 2 * W) cap <<= 1;
     for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
     __syncwarp();
-    rate_accumulate<true>(A, u, keys, sc, cm, cap - 1, lane, 32, nullptr, nullptr, nullptr, nullptr,
-                          nullptr, nullptr);
+    rate_flat(A, u, keys, sc, cm, cap - 1, 0, 32);
     __syncwarp();
     u64 prev = ~0ull;
     for (u32 r = 0; r < A.cnc; ++r) {
@@ -219,7 +179,6 @@ __device__ __forceinline__ u64 block_max_u64(u64 v, u64 *red) {
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
                                                         u32 cap_max, u32 *gtab) {
     extern __shared__ u32 dyn[];
-    __shared__ u32 sh_excl[RT_BLOCK], sh_c[RT_BLOCK], sh_s[RT_BLOCK], sh_inb[RT_BLOCK], sh_tot;
     __shared__ u64 red[33];
     u32 *keys, *sc, *cm;
     if (gtab) {
@@ -236,7 +195,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
         u64 W = 0;
         for (u64 j = A.toff[u] + threadIdx.x; j < A.toff[u + 1]; j += blockDim.x) {
             u32 h = A.touch[j];
-            W += A.off[h + 1] - A.off[h];
+            W += rated_len(A.off[h + 1] - A.off[h]);
         }
         W = warp_sum(W);
         if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long *)&Wsh, (unsigned long long)W);
@@ -248,8 +207,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
         cm = sc + cap;
         for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
         __syncthreads();
-        rate_accumulate<false>(A, u, keys, sc, cm, cap - 1, threadIdx.x, blockDim.x, sh_excl, nullptr, sh_c,
-                               sh_s, sh_inb, &sh_tot);
+        rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x);
         __syncthreads();
         u64 prev = ~0ull;
         for (u32 r = 0; r < A.cnc; ++r) {

@@ -4,6 +4,7 @@
 // one device arena: level l+1 is allocated on top of level l, so uncoarsening pops levels in LIFO
 // order. Stop rules follow sources/main.cu:358, 448, 495-500 and headers/defines.cuh:28-37.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -12,6 +13,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "axc_host.h"
 
 struct axc_ctx {
     axc::Ctx c;
@@ -26,6 +28,26 @@ struct Resolved {
     u32 omega, delta, max_parts, k, target, omega_c, cnc, rfr;
     int ipm;
     u64 seed;
+    int verbose;
+};
+
+// Phase log on stderr (-v 1 and up): synchronizes the stream, so it perturbs timing.
+struct PhaseLog {
+    Ctx &c;
+    int on;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double ms() {
+        cudaStreamSynchronize(c.stream);
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    template <class... A>
+    void operator()(const char *fmt, A... a) {
+        if (!on) return;
+        const double t = ms();
+        std::fprintf(stderr, "[axc %9.2f ms] ", t);
+        std::fprintf(stderr, fmt, a...);
+        std::fprintf(stderr, "  (arena %.2f GB, peak %.2f GB)\n", c.arena.top / 1e9, c.arena.peak / 1e9);
+    }
 };
 
 static int resolve(const axc_params *p, u32 n, Resolved &r) {
@@ -36,6 +58,7 @@ static int resolve(const axc_params *p, u32 n, Resolved &r) {
     r.rfr = p->rfr;
     r.ipm = p->ipm;
     r.seed = p->seed;
+    r.verbose = p->verbose;
     if (r.kway) {
         if (p->k == 0 || !(p->eps >= 0.0f)) return AXC_EINVAL;
         r.k = p->k;
@@ -106,10 +129,12 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
                           const float *d_w, u64 P_in, const Resolved &R, u32 *d_out, axc_stats *st,
                           cudaEvent_t ev_core) {
     const size_t base = c.arena.mark();
+    PhaseLog log{c, R.verbose};
     u32 *wfx = c.arena.alloc<u32>(e ? e : 1);
     compute_wfx(c, d_w, wfx, e);
     std::vector<DLevel> lv;
     lv.push_back(build_level0(c, n, e, d_off, d_pins, d_nsrc, P_in));
+    log("level 0 built: n %u, e %u, pins %llu", n, e, (unsigned long long)lv[0].P);
     if (st) st->pins = lv[0].P;
     if (ev_core) AXC_CUDA(cudaEventRecord(ev_core, c.stream));
     u32 K = 0;
@@ -130,9 +155,11 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
         u64 visits = 0;
         rating(c, cur, wfx, R.kway ? R.omega_c : R.omega, R.delta, R.cnc, pairs, scores, st ? &visits : nullptr);
         if (st) st->rating_pin_visits += visits;
+        log("level %u rated", l);
         u32 ng = matching(c, cur.n, R.cnc, pairs, scores, cur.nsize, cur.nin, R.kway ? R.omega_c : R.omega, R.delta, 32,
                           cur.groups);
         c.arena.release(tmp);
+        log("level %u matched: %u -> %u groups", l, cur.n, ng);
         const float ratio = (float)ng / (float)cur.n;
         if (R.kway && (ratio > 0.95f || ng < 1024)) {  // headers/defines.cuh:36-37
             deep_part = c.arena.alloc<u32>(cur.n ? cur.n : 1);
@@ -150,7 +177,9 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
         cur.ngroups = ng;
         DLevel nx = build_coarse(c, lv.back());
         lv.push_back(nx);
+        log("level %u built: n %u, pins %llu", l + 1, nx.n, (unsigned long long)nx.P);
     }
+    log("initial partition: %u parts at level %zu", K, lv.size() - 1);
     if (st) st->levels = (u32)lv.size();
     // uncoarsen and refine, popping levels
     RefineParams rp{K, R.omega, R.delta, !R.kway, R.rfr, R.seed};
@@ -175,6 +204,7 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
         if (l < deepest || refine_deepest) {
             u32 rr = refine_level(c, L, wfx, rp, part);
             if (st && l < 64) st->refine_rounds[l] = rr;
+            log("level %d refined: %u rounds", l, rr);
         }
         upper = part;
     }
@@ -182,6 +212,7 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
     if (!R.kway) merge_small_partitions(c, lv[0], final_part, K, R.omega, R.delta);
     const u32 Kp = zero_base(c, n, final_part, K);
     AXC_CUDA(cudaMemcpyAsync(d_out, final_part, (size_t)n * 4, cudaMemcpyDeviceToDevice, c.stream));
+    log("done: %u parts", Kp);
     c.arena.release(base);
     return Kp;
 }
@@ -361,6 +392,8 @@ int axc_partition_device(axc_ctx *ctx, const axc_hgraph *d_g, const axc_params *
         axc_stats *st = stats ? stats : &local;
         std::memset(st, 0, sizeof *st);
         c.launches = 0;
+        const size_t top0 = c.arena.top;
+        c.arena.peak = top0;
         cudaEvent_t e0, e1, ec;
         AXC_CUDA(cudaEventCreate(&e0));
         AXC_CUDA(cudaEventCreate(&e1));
@@ -378,6 +411,7 @@ int axc_partition_device(axc_ctx *ctx, const axc_hgraph *d_g, const axc_params *
         st->ms_core = mc;
         st->num_parts = Kp;
         st->kernel_launches = c.launches;
+        st->device_bytes_peak = c.arena.peak - top0;
         return AXC_OK;
     } catch (const std::exception &e) {
         cudaStreamSynchronize(c.stream);
@@ -421,11 +455,14 @@ static int validate_ids(const axc_hgraph *g) {
     return AXC_OK;
 }
 
-int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32_t *out_part, axc_stats *stats) {
-    if (!ctx || check_graph(g) || !p || (!out_part && g->n)) return AXC_EINVAL;
+}  // extern "C"
+
+namespace axc {
+// axc_partition on a given context (the caller serializes calls on it): upload, partition,
+// download and, when stats are wanted, the metrics of the result.
+int partition_host(Ctx &c, const axc_hgraph *g, const axc_params *p, uint32_t *out_part, axc_stats *stats) {
+    if (check_graph(g) || !p || (!out_part && g->n)) return AXC_EINVAL;
     if (int rc = validate_ids(g)) return rc;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    Ctx &c = ctx->c;
     try {
         Resolved R;
         int rc = resolve(p, g->n, R);
@@ -435,6 +472,8 @@ int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32
         axc_stats *st = stats ? stats : &local;
         std::memset(st, 0, sizeof *st);
         c.launches = 0;
+        const size_t top0 = c.arena.top;
+        c.arena.peak = top0;
         cudaEvent_t e0, e1, ec;
         AXC_CUDA(cudaEventCreate(&e0));
         AXC_CUDA(cudaEventCreate(&e1));
@@ -456,6 +495,7 @@ int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32
         st->ms_core = mc;
         st->num_parts = Kp;
         st->kernel_launches = c.launches;
+        st->device_bytes_peak = c.arena.peak - top0;
         if (stats) {
             // metrics of the result on the deduplicated graph (untimed, like sources/main.cu:917-928)
             DLevel L0 = build_level0(c, g->n, g->e, d.hedge_off, d.pins, d.src_count, P);
@@ -474,8 +514,108 @@ int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32
     } catch (const std::exception &e) {
         cudaStreamSynchronize(c.stream);
         c.arena.release(0);
-        return guard(ctx, e);
+        if (auto *x = dynamic_cast<const Error *>(&e)) {
+            c.last_error = x->what();
+            return x->code;
+        }
+        c.last_error = e.what();
+        return AXC_EINTERNAL;
     }
+}
+
+// ---------------------------------------------------------------- lanes (batching and serving)
+// A lane is a context without an arena of its own: a stream, a status word, a pinned staging
+// buffer and a scan state. Each job gets a device arena from the stream-ordered allocator on the
+// lane's stream, sized by the caller, and returns it when it finishes.
+struct Lane {
+    Ctx c;
+};
+
+int ctx_device(axc_ctx *ctx) { return ctx ? ctx->c.device : 0; }
+
+size_t device_free_bytes(int device) {
+    size_t fr = 0, tot = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+    return fr;
+}
+
+void lane_destroy(Lane *l) {
+    if (!l) return;
+    Ctx &c = l->c;
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    if (c.d_status) cudaFree(c.d_status);
+    if (c.h_pinned) cudaFreeHost(c.h_pinned);
+    scan_state_destroy(c);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    for (cudaEvent_t e : c.prof_ev) cudaEventDestroy(e);
+    delete l;
+}
+
+Lane *lane_create(int device, int *rc) {
+    auto *l = new Lane();
+    Ctx &c = l->c;
+    try {
+        c.device = device;
+        AXC_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        AXC_CUDA(cudaGetDeviceProperties(&prop, device));
+        c.sms = prop.multiProcessorCount;
+        c.smem_optin = prop.sharedMemPerBlockOptin;
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+        c.coop_supported = coop;
+        AXC_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        AXC_CUDA(cudaMalloc(&c.d_status, 256));
+        AXC_CUDA(cudaMemset(c.d_status, 0, 256));
+        AXC_CUDA(cudaHostAlloc((void **)&c.h_pinned, 4096, cudaHostAllocDefault));
+        scan_state_create(c, 1u << 18);
+        // freed job arenas stay in the pool for the next job instead of going back to the driver
+        cudaMemPool_t pool;
+        AXC_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        u64 keep = ~0ull;
+        AXC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        *rc = AXC_OK;
+    } catch (const std::exception &e) {
+        auto *x = dynamic_cast<const Error *>(&e);
+        *rc = x ? x->code : AXC_ECUDA;
+        lane_destroy(l);
+        return nullptr;
+    }
+    return l;
+}
+
+// One job on the lane in a fresh arena of `arena_bytes`. AXC_ENOMEM when the arena cannot be had
+// or turns out too small.
+int lane_partition(Lane *l, size_t arena_bytes, const axc_hgraph *g, const axc_params *p, uint32_t *out_part,
+                   axc_stats *stats, std::string *err) {
+    Ctx &c = l->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return AXC_ECUDA;
+    void *mem = nullptr;
+    if (cudaMallocAsync(&mem, arena_bytes, c.stream) != cudaSuccess) {
+        cudaGetLastError();
+        if (err) *err = "device arena of " + std::to_string(arena_bytes) + " bytes not available";
+        return AXC_ENOMEM;
+    }
+    c.arena.base = (char *)mem;
+    c.arena.cap = arena_bytes;
+    c.arena.top = 0;
+    c.arena.peak = 0;
+    const int rc = partition_host(c, g, p, out_part, stats);
+    if (rc && err) *err = c.last_error;
+    cudaFreeAsync(mem, c.stream);
+    cudaStreamSynchronize(c.stream);
+    c.arena = Arena();
+    return rc;
+}
+
+}  // namespace axc
+
+extern "C" {
+
+int axc_partition(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint32_t *out_part, axc_stats *stats) {
+    if (!ctx) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return partition_host(ctx->c, g, p, out_part, stats);
 }
 
 int axc_evaluate(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, const uint32_t *part, axc_stats *stats) {

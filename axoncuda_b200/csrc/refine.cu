@@ -216,36 +216,62 @@ __global__ void k_gain_bounds(u32 n, u32 K, const u64 *__restrict__ toff, const 
         atomicMax(wmax, (unsigned long long)ws);
     }
 }
-__device__ __forceinline__ u32 table_cap(u64 work, u32 cap_max) {
+__host__ __device__ __forceinline__ u32 table_cap(u64 work, u32 cap_max) {
     u32 cap = 32;
     while (cap < 2 * work && cap < cap_max) cap <<= 1;
     return cap;
 }
 
-// Accumulate node u's adjacency to other partitions into (keys, conn, dconn); saving and the
-// total incident weight are summed by the caller over threads [0, nt).
-__device__ __forceinline__ void gain_accumulate(const GainArgs &A, u32 u, u32 p, u32 *keys,
-                                                unsigned long long *conn, u32 *dconn, u32 mask, u32 t, u32 nt,
-                                                i64 &saving, i64 &wtot) {
-    const u64 t0 = A.toff[u], t1 = A.toff[u + 1];
-    const u32 nin_u = A.nin[u];
-    for (u64 j = t0; j < t1; ++j) {
-        const u32 h = A.touch[j];
-        const bool inb = (j - t0) < nin_u;
-        const u32 w = A.wfx[h];
-        const u64 a = A.off[h];
-        const u32 lm = A.lam[h];
-        if (t == 0) wtot += w;
-        for (u32 i = t; i < lm; i += nt) {
-            const u32 q = A.cpart[a + i];
+// Accumulate node u's adjacency to other partitions into (keys, conn, dconn). Warp-cooperative:
+// the calling warp takes the node's incidences in batches of 32 starting at `first`, every
+// `stride` entries. A batch's hyperedge metadata loads in parallel; its census entries are then
+// flattened across the lanes (each lane finds its entry's hyperedge by a 5-step search over the
+// prefix of the batch's lambdas). saving and wtot are per-lane partial sums.
+__device__ __forceinline__ void gain_flat(const GainArgs &A, u32 u, u32 p, u32 *keys, unsigned long long *conn,
+                                          u32 *dconn, u32 mask, u32 first, u32 stride, i64 &saving, i64 &wtot) {
+    const u32 lane = threadIdx.x & 31u;
+    const u64 t0 = A.toff[u];
+    const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
+    for (u32 jb = first; jb < deg; jb += stride) {
+        const u32 j = jb + lane;
+        const bool has = j < deg;
+        const u32 h = has ? A.touch[t0 + j] : 0;
+        const u32 lm = has ? A.lam[h] : 0;
+        const u32 wh = has ? A.wfx[h] : 0;
+        const u64 ah = has ? A.off[h] : 0;
+        const u32 ib = (has && j < nin_u) ? 1u : 0u;
+        wtot += wh;
+        u32 x = lm;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - lm;
+        const u32 chunk = (deg - jb) < 32 ? (deg - jb) : 32;
+        for (u32 fb = 0; fb < total; fb += 32) {
+            const u32 f = fb + lane;
+            u32 lo = 0, hi = chunk - 1;
+            for (int it = 0; it < 5; ++it) {
+                const u32 mid = (lo + hi + 1) >> 1;
+                const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
+                if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
+            }
+            const u32 eo = __shfl_sync(0xFFFFFFFFu, excl, lo);
+            const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, lo);
+            const u32 wo = __shfl_sync(0xFFFFFFFFu, wh, lo);
+            const u32 io = __shfl_sync(0xFFFFFFFFu, ib, lo);
+            if (f >= total) continue;
+            const u64 k = ao + (f - eo);
+            const u32 q = A.cpart[k];
             if (q == p) {
-                saving += leave_gain(A.encourage, w, A.ccnt[a + i]);
+                saving += leave_gain(A.encourage, wo, A.ccnt[k]);
                 continue;
             }
             const u32 slot = hash_find_or_insert(keys, mask, q);
             if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
-            atomicAdd(&conn[slot], (unsigned long long)w);
-            if (inb && A.cdcnt[a + i] > 0) atomicAdd(&dconn[slot], 1u);
+            atomicAdd(&conn[slot], (unsigned long long)wo);
+            if (io && A.cdcnt[k] > 0) atomicAdd(&dconn[slot], 1u);
         }
     }
 }
@@ -285,6 +311,7 @@ constexpr u32 GN_WARP_W = 128;
 constexpr u32 GN_WARPS = 4;
 constexpr u32 GN_BLOCK = 256;
 constexpr u32 GN_BLOCK_W = 4096;
+constexpr u32 GN_WARP_DEG = 256;  // incidences one warp takes; more go to a block
 
 __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const u32 *__restrict__ list, u32 nl,
                                                              const u64 *__restrict__ work) {
@@ -301,52 +328,7 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const 
     for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
     __syncwarp();
     i64 saving = 0, wtot = 0;
-    // 32 incident hyperedges at a time: their metadata loads in parallel, then their census
-    // entries are flattened across the lanes (owner found by a 5-step search over the prefix)
-    const u64 t0 = A.toff[u];
-    const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
-    for (u32 jb = 0; jb < deg; jb += 32) {
-        const u32 j = jb + lane;
-        const bool has = j < deg;
-        const u32 h = has ? A.touch[t0 + j] : 0;
-        const u32 lm = has ? A.lam[h] : 0;
-        const u32 wh = has ? A.wfx[h] : 0;
-        const u64 ah = has ? A.off[h] : 0;
-        const u32 ib = (has && j < nin_u) ? 1u : 0u;
-        wtot += wh;
-        u32 x = lm;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-            if ((int)lane >= o) x += y;
-        }
-        const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - lm;
-        const u32 chunk = (deg - jb) < 32 ? (deg - jb) : 32;
-        for (u32 fb = 0; fb < total; fb += 32) {
-            const u32 f = fb + lane;
-            u32 lo = 0, hi = chunk - 1;
-            for (int it = 0; it < 5; ++it) {
-                const u32 mid = (lo + hi + 1) >> 1;
-                const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
-                if (lo < hi) { if (em <= f) lo = mid; else hi = mid - 1; }
-            }
-            const u32 eo = __shfl_sync(0xFFFFFFFFu, excl, lo);
-            const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, lo);
-            const u32 wo = __shfl_sync(0xFFFFFFFFu, wh, lo);
-            const u32 io = __shfl_sync(0xFFFFFFFFu, ib, lo);
-            if (f >= total) continue;
-            const u64 k = ao + (f - eo);
-            const u32 q = A.cpart[k];
-            if (q == p) {
-                saving += leave_gain(A.encourage, wo, A.ccnt[k]);
-                continue;
-            }
-            const u32 slot = hash_find_or_insert(keys, cap - 1, q);
-            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
-            atomicAdd(&conn[slot], (unsigned long long)wo);
-            if (io && A.cdcnt[k] > 0) atomicAdd(&dconn[slot], 1u);
-        }
-    }
+    gain_flat(A, u, p, keys, conn, dconn, cap - 1, 0, 32, saving, wtot);
     saving = warp_sum(saving);
     wtot = warp_sum(wtot);
     __syncwarp();
@@ -392,7 +374,7 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 
         for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
         __syncthreads();
         i64 saving = 0, wtot = 0;
-        gain_accumulate(A, u, p, keys, conn, dconn, cap - 1, threadIdx.x, blockDim.x, saving, wtot);
+        gain_flat(A, u, p, keys, conn, dconn, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x, saving, wtot);
         saving = warp_sum(saving);
         wtot = warp_sum(wtot);
         if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = saving; red[1][threadIdx.x >> 5] = wtot; }
@@ -432,10 +414,22 @@ __global__ void k_list_degree(const u32 *__restrict__ list, u32 nl, const u64 *_
     d = warp_sum(d);
     if ((threadIdx.x & 31) == 0 && d) atomicAdd(out, (unsigned long long)d);
 }
-__global__ void k_tier(u32 n, const u64 *__restrict__ work, u64 lo, u64 hi, u32 *__restrict__ flag) {
+__global__ void k_list_max(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ v,
+                           unsigned long long *__restrict__ out) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 m = i < nl ? v[list[i]] : 0;
+    m = warp_max_u64(m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, (unsigned long long)m);
+}
+// Gain tiers: 0 = one warp (small table, at most GN_WARP_DEG incidences), 1 = one block with the
+// table in shared memory, 2 = one block with the table in global scratch.
+__global__ void k_tier(u32 n, const u64 *__restrict__ work, const u64 *__restrict__ toff, u32 tier,
+                       u32 *__restrict__ flag) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
-    // the first tier (lo == 0) also takes nodes without incident hyperedges
-    if (u < n) flag[u] = ((lo == 0 || work[u] > lo) && work[u] <= hi) ? 1u : 0u;
+    if (u >= n) return;
+    const u64 wk = work[u], deg = toff[u + 1] - toff[u];
+    const u32 t = wk > GN_BLOCK_W ? 2u : ((wk <= GN_WARP_W && deg <= GN_WARP_DEG) ? 0u : 1u);
+    flag[u] = t == tier ? 1u : 0u;
 }
 
 // ------------------------------------------------------------------ ranking
@@ -566,16 +560,40 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__rest
     if (lane == 0) cascade_sweep(A, h, mvs[w], m, tk[w], tc[w], td[w], cap - 1);
 }
 
-// Hyperedges with many movers: one block at a time per hyperedge, movers and table in this
-// block's slice of a scratch region sized by the level's largest hyperedge.
+// Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
+__device__ void block_bitonic_u64(u64 *buf, u32 P) {
+    for (u32 k = 2; k <= P; k <<= 1) {
+        for (u32 j = k >> 1; j > 0; j >>= 1) {
+            for (u32 i = threadIdx.x; i < P; i += blockDim.x) {
+                const u32 ixj = i ^ j;
+                if (ixj > i) {
+                    const u64 x = buf[i], y = buf[ixj];
+                    if ((x > y) == ((i & k) == 0)) {
+                        buf[i] = y;
+                        buf[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+constexpr u32 CB_SMEM = 4096;  // movers sorted in shared memory (32 KB); larger sets sort in scratch
+
+// Hyperedges with many movers: one block at a time per hyperedge. Movers are sorted by rank with
+// a bitonic sort, in shared memory when the hyperedge has at most CB_SMEM pins, else in this
+// block's slice of a scratch region (mv_cap entries, a power of two >= the largest hyperedge).
 __global__ void k_cascade_big(CascadeArgs A, const u32 *__restrict__ list, const u32 *__restrict__ nl, u64 *scratch_mv,
                               u32 *scratch_tab, u64 mv_cap, u64 tab_cap) {
+    __shared__ u64 smv[CB_SMEM];
     __shared__ u32 cntm;
-    u64 *mvs = scratch_mv + (u64)blockIdx.x * mv_cap;
+    u64 *gmv = scratch_mv + (u64)blockIdx.x * mv_cap;
     for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
         const u32 h = list[idx];
         const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
         const u32 lm = A.lam[h];
+        u64 *mvs = (b - a) <= CB_SMEM ? smv : gmv;
         if (threadIdx.x == 0) cntm = 0;
         __syncthreads();
         for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
@@ -584,14 +602,11 @@ __global__ void k_cascade_big(CascadeArgs A, const u32 *__restrict__ list, const
         }
         __syncthreads();
         const u32 m = cntm;
-        // sort by rank: odd-even transposition (m is bounded by the hyperedge size)
-        for (u32 phase = 0; phase < m; ++phase) {
-            for (u32 i = 2 * threadIdx.x + (phase & 1); i + 1 < m; i += 2 * blockDim.x) {
-                u64 x = mvs[i], y = mvs[i + 1];
-                if (x > y) { mvs[i] = y; mvs[i + 1] = x; }
-            }
-            __syncthreads();
-        }
+        u32 P = 1;
+        while (P < m) P <<= 1;
+        for (u32 i = m + threadIdx.x; i < P; i += blockDim.x) mvs[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_u64(mvs, P);
         u32 cap = 32;
         while (cap < 2 * (lm + 2 * m)) cap <<= 1;
         u32 *tk = scratch_tab + (u64)blockIdx.x * tab_cap, *tc = tk + cap, *td = tc + cap;
@@ -729,22 +744,41 @@ __device__ __forceinline__ bool best_better(const Best &b, const Best &a) {  // 
     if (a.g != b.g) return b.g > a.g;
     return b.r < a.r;
 }
+__device__ __forceinline__ Best best_pick(const Best &a, const Best &b) {  // the better one; r = ~0 is empty
+    if (b.r == 0xFFFFFFFFu) return a;
+    if (a.r == 0xFFFFFFFFu) return b;
+    return best_better(b, a) ? b : a;
+}
+__device__ __forceinline__ Best warp_best_prefix(Best b) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        Best c;
+        c.ok = __shfl_xor_sync(0xFFFFFFFFu, b.ok, o);
+        c.vs = __shfl_xor_sync(0xFFFFFFFFu, b.vs, o);
+        c.g = __shfl_xor_sync(0xFFFFFFFFu, b.g, o);
+        c.r = __shfl_xor_sync(0xFFFFFFFFu, b.r, o);
+        b = best_pick(b, c);
+    }
+    return b;
+}
+// best_better is a strict total order (ties end on the rank), so the tree reduction picks the
+// same prefix as a sequential scan would.
 __global__ void k_best(const i64 *__restrict__ G, const i64 *__restrict__ Vs, const i64 *__restrict__ Vi,
                        const u32 *__restrict__ dM, Best *__restrict__ out) {
-    __shared__ Best sh[256];
+    __shared__ Best sh[32];
     Best b{0, 0, 0, 0xFFFFFFFFu};
     const u32 M = *dM;
     for (u32 r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
         Best c{Vi ? (Vi[r] == 0 ? 1u : 0u) : 1u, Vs[r], G[r], r};
-        if (b.r == 0xFFFFFFFFu || best_better(c, b)) b = c;
+        b = best_pick(b, c);
     }
-    sh[threadIdx.x] = b;
+    b = warp_best_prefix(b);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = b;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        Best x = sh[0];
-        for (u32 i = 1; i < blockDim.x; ++i)
-            if (sh[i].r != 0xFFFFFFFFu && (x.r == 0xFFFFFFFFu || best_better(sh[i], x))) x = sh[i];
-        out[blockIdx.x] = x;
+    if (threadIdx.x < 32) {
+        Best x = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : Best{0, 0, 0, 0xFFFFFFFFu};
+        x = warp_best_prefix(x);
+        if (threadIdx.x == 0) out[blockIdx.x] = x;
     }
 }
 __global__ void k_best_final(const Best *__restrict__ in, u32 nb, const i64 *__restrict__ Vi, Best *__restrict__ out,
@@ -789,7 +823,8 @@ struct LevelPrep {
     u32 ncount[3] = {0, 0, 0};
     u64 *work = nullptr;     // per-node table bound of the gains
     u64 heavy_work_max = 0;  // largest gain-work bound of the heavy tier
-    u64 gain_bound = 0;      // no gain exceeds this (sum of incident weights)
+    u64 block_work_max = 0;  // largest gain-work bound of the block tier (sizes its shared table)
+    u64 gain_bound = 0;     // no gain exceeds this (sum of incident weights)
     u64 max_len = 0;         // largest hyperedge
     u64 dst_pins = 0;        // destination pins (bounds the inbound events: 2 per pin)
     u64 tier_deg[3] = {0, 0, 0};  // incidence entries of each gain tier (kernel timer only)
@@ -825,14 +860,19 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
         AXC_CUDA(cudaMemsetAsync(wm, 0, 8, c.stream));
         LAUNCH(c, k_gain_bounds, cdiv((u64)n * 32, 256), 256, 0, n, K, L.toff, L.touch, L.off, wfx, work, wm);
         u32 *flag = c.arena.alloc<u32>(n);
-        const u64 lim[4] = {0, GN_WARP_W, GN_BLOCK_W, ~0ull};
-        for (int t = 0; t < 3; ++t) {
+        for (u32 t = 0; t < 3; ++t) {
             lp.ntier[t] = c.arena.alloc<u32>(n);
-            LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, work, lim[t], lim[t + 1], flag);
+            LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, work, L.toff, t, flag);
             lp.ncount[t] = compact_indices(c, flag, lp.ntier[t], n);
         }
         lp.gain_bound = fetch1(c, (const u64 *)wm);
         if (lp.ncount[2]) lp.heavy_work_max = reduce_max_u64(c, work, n);
+        if (lp.ncount[1]) {
+            unsigned long long *bm = c.arena.alloc<unsigned long long>(1);
+            AXC_CUDA(cudaMemsetAsync(bm, 0, 8, c.stream));
+            LAUNCH(c, k_list_max, cdiv(lp.ncount[1], 256), 256, 0, lp.ntier[1], lp.ncount[1], work, bm);
+            lp.block_work_max = fetch1(c, (const u64 *)bm);
+        }
         if (c.profiling("k_gain_warp") || c.profiling("k_gain_block")) {
             unsigned long long *dg = c.arena.alloc<unsigned long long>(3);
             AXC_CUDA(cudaMemsetAsync(dg, 0, 24, c.stream));
@@ -880,8 +920,12 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
     if (c.profiling("k_gain_warp") && lp.ncount[0]) c.prof_bytes += gain_bytes(lp, 0);
     if (c.profiling("k_gain_block")) c.prof_bytes += gain_bytes(lp, 1) + gain_bytes(lp, 2);
     LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
-    LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, 2 * GN_BLOCK_W * 16, A, lp.ntier[1], lp.ncount[1], 2 * GN_BLOCK_W,
-           (u32 *)nullptr, lp.work);
+    if (lp.ncount[1]) {
+        // shared table sized by the tier's largest bound (16 B per slot)
+        const u32 cap1 = table_cap(lp.block_work_max, 2 * GN_BLOCK_W);
+        LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, cap1 * 16, A, lp.ntier[1], lp.ncount[1], cap1, (u32 *)nullptr,
+               lp.work);
+    }
     if (lp.ncount[2]) {
         size_t m = c.arena.mark();
         u32 cap = 64;
@@ -1011,7 +1055,8 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1);
         if (L.e) LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
         // scratch per resident block, sized by the level's largest hyperedge
-        const u64 mv_cap = lp.max_len ? lp.max_len : 1;
+        u64 mv_cap = 1;
+        while (mv_cap < lp.max_len) mv_cap <<= 1;
         u64 cap = 32;
         while (cap < 2 * (3 * mv_cap)) cap <<= 1;
         const u32 grid = (u32)c.sms;

@@ -276,18 +276,33 @@ def run_ours(args, world, rank, local):
     return out, g, p, part
 
 
-def cpu_port_baseline(g, p, budget_s: float = 30.0) -> dict:
+CPU_SAMPLE_PINS = 5_000_000  # above this the CPU baseline times a smaller instance of the generator
+
+
+def cpu_sample(name: str, g, p):
+    """The workload itself when the oracle finishes it in seconds, else a smaller instance of the same
+    generator with the same parameters (the large SNN at 20 x 500 neurons), with its description."""
+    import axoncuda_b200 as ax
+    if g.P > CPU_SAMPLE_PINS and name.startswith("snn-1m"):
+        gs = ax.gen_snn(20, 500, 256, 0.8, 2048, 0.7, 2)
+        return gs, (f"one full step of the same generator at 20 x 500 neurons ({gs.P} pins; the workload has "
+                    f"{g.P}), same parameters")
+    return g, f"one full step of the workload ({g.P} pins)"
+
+
+def cpu_port_baseline(g, p, name: str) -> dict:
     from oracle import oracle as O
+    gs, what = cpu_sample(name, g, p)
     t0 = time.perf_counter()
     if p.mode == 0:
-        O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 0, omega=p.omega, delta=p.delta, max_parts=p.max_parts,
+        O.partition(gs.n, gs.off, gs.pins, gs.nsrc, gs.w, 0, omega=p.omega, delta=p.delta, max_parts=p.max_parts,
                     cnc=p.cnc, rfr=p.rfr, ipm=p.ipm, seed=p.seed)
     else:
-        O.partition(g.n, g.off, g.pins, g.nsrc, g.w, 1, k=p.k, eps=p.eps, cnc=p.cnc, rfr=p.rfr, seed=p.seed)
+        O.partition(gs.n, gs.off, gs.pins, gs.nsrc, gs.w, 1, k=p.k, eps=p.eps, cnc=p.cnc, rfr=p.rfr, seed=p.seed)
     dt = time.perf_counter() - t0
-    return {"value": g.P / dt, "unit": "pins/s", "cores": 1, "kind": "port",
-            "sample": f"one full step of the workload ({g.P} pins) through the oracle's single-threaded "
-                      f"C++ restatement of the whole partitioner, {dt:.2f} s"}
+    return {"value": gs.P / dt, "unit": "pins/s", "cores": 1, "kind": "port",
+            "sample": f"{what} through the oracle's single-threaded C++ restatement of the whole partitioner, "
+                      f"{dt:.2f} s"}
 
 
 def run_reference(args):
@@ -310,11 +325,20 @@ def run_reference(args):
             conn = None
             for i in range(args.warmup + args.steps):
                 pf = os.path.join(td, "out.part")
-                r = subprocess.run([exe, "-r", path, *flags, "-p", pf], capture_output=True, text=True, cwd=td)
+                try:
+                    r = subprocess.run([exe, "-r", path, *flags, "-p", pf], capture_output=True, text=True, cwd=td,
+                                       timeout=args.ref_timeout)
+                except subprocess.TimeoutExpired:
+                    line["unavailable"] = f"reference did not finish one partition within {args.ref_timeout:.0f} s"
+                    return line
                 if r.returncode != 0:
-                    line["unavailable"] = f"reference exited {r.returncode}: {r.stderr.strip()[-200:]}"
+                    tail = (r.stderr.strip() or r.stdout.strip())[-200:]
+                    line["unavailable"] = f"reference exited {r.returncode}: {tail}"
                     return line
                 m = re.search(r"Total host execution time: ([0-9.]+) ms", r.stdout)
+                if m is None:
+                    line["unavailable"] = "reference printed no 'Total host execution time'"
+                    return line
                 if i >= args.warmup:
                     times.append(float(m.group(1)))
                 mc = re.search(r"Connectivity:\s+([0-9.]+)", r.stdout)
@@ -330,11 +354,146 @@ def run_reference(args):
             return line
     # k-way: the reference needs the external Mt-KaHyPar binary (sources/init_part.cu:891-906), which
     # is not installable offline; time the oracle's CPU port instead.
-    cb = cpu_port_baseline(g, p)
+    cb = cpu_port_baseline(g, p, args.workload)
     line.update({"value": cb["value"], "ms_per_step": g.P / cb["value"] * 1e3, "cpu_baseline": cb,
                  "e2e": {"value": cb["value"], "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "note": "reference k-way needs mtkahypar (absent); CPU port of the oracle timed instead"})
     return line
+
+
+def batch_jobs(count: int = 256, seed0: int = 100):
+    """The batched workload: `count` hypergraphs, seeds seed0.., alternately from the circuit and the
+    layered-SNN generator, nodes log-uniform in [1e3, 1e5] (nets in proportion), k-way with k drawn
+    from {2, 8, 32}, eps 0.03."""
+    import axoncuda_b200 as ax
+    rng = np.random.default_rng(seed0)
+    jobs = []
+    for i in range(count):
+        s = seed0 + i
+        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e5)))))
+        k = int(rng.choice([2, 8, 32]))
+        if i % 2 == 0:
+            g = ax.gen_circuit(n, int(1.1 * n), 2, 64, 2.5, 0.9, 0.02, s)
+        else:
+            g = ax.gen_snn(8, max(n // 8, 65), 64, 0.0, 0, 1.0, s)
+        jobs.append((g, ax.params_kway(k, 0.03, cnc=4, rfr=16)))
+    return jobs
+
+
+def serve_requests(count: int, max_pins: float, seed: int = 7):
+    """The served workload: requests with pin counts log-uniform in [1e4, max_pins], half from the
+    circuit generator and half from the lognormal-fan-out SNN generator; half INCC (omega 256,
+    delta 2048), half k-way with k in {2, 16, 64}, eps 0.03."""
+    import axoncuda_b200 as ax
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        pins = float(np.exp(rng.uniform(np.log(1e4), np.log(max_pins))))
+        if i % 2 == 0:  # circuit: about 4.4 pins per net, 1.1 nets per node
+            n = max(int(pins / 4.85), 1000)
+            g = ax.gen_circuit(n, int(1.1 * n), 2, 64, 2.5, 0.9, 0.02, 1000 + i)
+        else:  # SNN, 20 layers, fan-out median 256: about 350 pins per neuron
+            width = max(int(pins / (20 * 350)), 64)
+            g = ax.gen_snn(20, width, 256, 0.8, 2048, 0.7, 1000 + i)
+        if rng.random() < 0.5:
+            p = ax.params_incc(256, 2048, 1048576, cnc=4, rfr=16)
+        else:
+            p = ax.params_kway(int(rng.choice([2, 16, 64])), 0.03, cnc=4, rfr=16)
+        reqs.append((g, p))
+    return reqs
+
+
+def percentiles(xs):
+    xs = np.asarray(xs, dtype=np.float64)
+    return {"p50_ms": float(np.percentile(xs, 50)), "p99_ms": float(np.percentile(xs, 99)),
+            "mean_ms": float(xs.mean())}
+
+
+def run_batch(args) -> dict:
+    """jobs/s of the batched workload through the executor's lanes (axc_partition_batch) against a
+    one-at-a-time loop of axc_partition over the same jobs; both from host buffers to host results."""
+    import axoncuda_b200 as ax
+    jobs = batch_jobs(args.batch_jobs)
+    pins = sum(g.P for g, _ in jobs)
+    with ax.Context(0, 2 << 30) as seq:
+        for g, p in jobs[:4]:
+            seq.partition(g, p)  # warm-up: module load, first allocations
+        t0 = time.perf_counter()
+        solo = [seq.partition(g, p)[0] for g, p in jobs]
+        t_seq = time.perf_counter() - t0
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(args.lanes, int(args.budget_gb * (1 << 30)))
+        srv.partition_batch(jobs[:args.lanes])  # warm-up: lanes, graphs of the first levels
+        with Clocks(0) as clk:
+            t0 = time.perf_counter()
+            res = srv.partition_batch(jobs)
+            t_bat = time.perf_counter() - t0
+    same = sum(int(np.array_equal(r[0], s)) for r, s in zip(res, solo))
+    lat = [st.ms_queued + st.ms_run for _, st in res]
+    return {"metric": "jobs/s batched (256 mixed k-way jobs)", "value": len(jobs) / t_bat, "unit": "jobs/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic (seeded generators)",
+            "config": {"workload": "batch-256", "jobs": len(jobs), "pins": pins, "lanes": args.lanes,
+                       "budget_gb": args.budget_gb},
+            "sequential": {"value": len(jobs) / t_seq, "unit": "jobs/s", "seconds": t_seq},
+            "speedup_vs_sequential": t_seq / t_bat, "seconds": t_bat, "pins_per_s": pins / t_bat,
+            "identical_to_sequential": f"{same}/{len(jobs)}",
+            "valid": f"{sum(int(st.valid) for _, st in res)}/{len(jobs)}",
+            "latency_in_batch": percentiles(lat), "clocks": clk.summary()}
+
+
+def run_serve(args) -> dict:
+    """A Poisson stream of requests through axc_submit / axc_poll with continuous batching, against a
+    FIFO single server running the same requests one at a time (its latencies follow from the
+    measured service times and the same arrival times)."""
+    import axoncuda_b200 as ax
+    reqs = serve_requests(args.serve_requests, args.serve_max_pins)
+    pins = sum(g.P for g, _ in reqs)
+    with ax.Context(0, int(args.seq_arena_gb * (1 << 30))) as seq:
+        seq.partition(*reqs[0])  # warm-up
+        service = []
+        for g, p in reqs:
+            t0 = time.perf_counter()
+            seq.partition(g, p)
+            service.append(time.perf_counter() - t0)
+    cap = len(reqs) / sum(service)
+    rate = args.serve_load * cap  # arrivals per second, a multiple of the sequential capacity
+    rng = np.random.default_rng(11)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    # the single server: FIFO, one request at a time
+    t, seq_lat = 0.0, []
+    for a, s in zip(arrivals, service):
+        t = max(t, a) + s
+        seq_lat.append((t - a) * 1e3)
+    seq_span = t - arrivals[0]
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(args.lanes, int(args.budget_gb * (1 << 30)))
+        srv.partition_batch(reqs[:args.lanes])  # warm-up
+        done = {}
+        ids = []
+        with Clocks(0) as clk:
+            t0 = time.perf_counter()
+            for a, (g, p) in zip(arrivals, reqs):
+                wait = t0 + (a - arrivals[0]) - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                ids.append(srv.submit(g, p))
+            for i, (jid, (g, _)) in enumerate(zip(ids, reqs)):
+                done[i] = srv.poll(jid, g.n)
+            span = time.perf_counter() - t0
+    lat = [done[i][1].ms_queued + done[i][1].ms_run for i in range(len(reqs))]
+    return {"metric": "jobs/s served (Poisson stream, continuous batching)", "value": len(reqs) / span,
+            "unit": "jobs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": "serve-poisson", "requests": len(reqs), "pins": pins,
+                       "pins_per_request": f"log-uniform in [1e4, {args.serve_max_pins:.0e}]",
+                       "arrival_rate_per_s": rate, "load_vs_sequential_capacity": args.serve_load,
+                       "lanes": args.lanes, "budget_gb": args.budget_gb},
+            "latency": percentiles(lat), "seconds": span,
+            "sequential": {"value": len(reqs) / seq_span, "unit": "jobs/s", "capacity_jobs_per_s": cap,
+                           "latency": percentiles(seq_lat)},
+            "speedup_vs_sequential": (len(reqs) / span) / (len(reqs) / seq_span),
+            "valid": f"{sum(int(done[i][1].valid) for i in range(len(reqs)))}/{len(reqs)}",
+            "clocks": clk.summary()}
 
 
 def main():
@@ -346,7 +505,21 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-kernel", default=ROOFLINE_KERNEL)
+    ap.add_argument("--ref-timeout", type=float, default=900.0,
+                    help="seconds one reference partition may take before its arm reports unavailable")
+    ap.add_argument("--mode", default="partition", choices=["partition", "batch", "serve"],
+                    help="partition: one hypergraph per step (the headline); batch / serve: many jobs")
+    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--batch-jobs", type=int, default=256)
+    ap.add_argument("--serve-requests", type=int, default=120)
+    ap.add_argument("--serve-max-pins", type=float, default=2e7)
+    ap.add_argument("--serve-load", type=float, default=2.0)
+    ap.add_argument("--seq-arena-gb", type=float, default=24.0)
     args = ap.parse_args()
+    if args.mode != "partition":
+        print(json.dumps(run_batch(args) if args.mode == "batch" else run_serve(args)), flush=True)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank == 0:
@@ -356,7 +529,7 @@ def main():
     out, g, p, part = run_ours(args, world, rank, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_port_baseline(g, p)
+            out["cpu_baseline"] = cpu_port_baseline(g, p, args.workload)
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist

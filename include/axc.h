@@ -79,6 +79,10 @@ typedef struct {
 
 #define AXC_MAX_CANDIDATES 16u   /* headers/defines.cuh:49 */
 #define AXC_FIXED_POINT_SCALE 262144u
+/* Hyperedges with more pins than this take no part in the coarsening rating (they still count
+ * everywhere else). The reference rates through every hyperedge (kernels/coarsening.cu:76-202);
+ * its pair visits grow as |e|^2, which at 3e8 pins is what exhausts its neighbour lists. */
+#define AXC_RATE_MAX_LEN 128u
 
 typedef struct {
     uint32_t num_parts;        /* K' after zero-basing */
@@ -100,6 +104,9 @@ typedef struct {
     uint32_t level_nodes[64];
     uint32_t refine_rounds[64];
     uint64_t rating_pin_visits;  /* sum over rated nodes of incident pins visited */
+    uint64_t device_bytes_peak;  /* arena high-water mark of this call (bytes) */
+    double ms_queued;            /* submitted jobs: host time from submit to start on a lane */
+    double ms_run;               /* submitted jobs: host time from start to finish */
 } axc_stats;
 
 typedef struct axc_ctx axc_ctx;
@@ -189,15 +196,25 @@ int axc_gen_circuit(uint32_t n, uint32_t e, uint32_t smin, uint32_t smax, double
                     double p_local, double local_frac, uint64_t seed, axc_hgraph *out);
 
 /* ---- batching and serving -------------------------------------------------------------------------
- * Many independent jobs on one device. Jobs are uploaded, coarsened, partitioned and refined
- * with their level hierarchies resident in the context's arena; job-level work of concurrent jobs
- * overlaps on the device. Admission is by device-memory budget. There is no reference counterpart:
- * the reference partitions exactly one hypergraph per process (sources/main.cu:38). */
+ * Many independent jobs on one device, continuously batched. There is no reference counterpart:
+ * the reference partitions exactly one hypergraph per process (sources/main.cu:38).
+ * - The context runs `lanes` workers, each with its own stream, status word, scan state and host
+ *   thread, next to the context's own arena and stream.
+ * - A job takes a device arena of its estimated size from the stream-ordered allocator on its
+ *   lane's stream, and keeps its whole level hierarchy there until it finishes.
+ * - Admission: a queued job starts when a lane is free and its estimate fits in `device_budget`
+ *   minus what running jobs hold. Smaller jobs may start ahead of a larger one that does not fit
+ *   yet. A job larger than the whole budget runs alone.
+ * - A job that runs out of its arena is requeued once with twice the estimate.
+ * - Concurrent jobs overlap on the device; each result equals the same job run alone.
+ * Call axc_serve_configure before the first submit; without it there is 1 lane and a budget of
+ * half the free device memory at the first submit. */
+int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_budget);
 int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint64_t *job_id);
 /* Wait up to timeout_ms (<0: forever) for a job; copies its partition into out_part[n]. */
 int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms);
-/* Partition `count` jobs as one batch (one launch sequence shared by all jobs). out_parts[i]
- * points at a host buffer of g[i].n entries. */
+/* Partition `count` jobs through the same lanes (submit all, then wait for all). out_parts[i]
+ * points at a host buffer of g[i].n entries; stats may be NULL. Returns the first failing status. */
 int axc_partition_batch(axc_ctx *ctx, uint32_t count, const axc_hgraph *g, const axc_params *p,
                         uint32_t *const *out_parts, axc_stats *stats);
 

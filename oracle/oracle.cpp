@@ -11,6 +11,7 @@
 // nondeterministic under atomics, and its k-way initial partition is the external Mt-KaHyPar);
 // for those the oracle is the specification the GPU path must reproduce bit for bit.
 #include "oracle.h"
+#include "../include/axc.h"  // public constants the restatement shares (AXC_RATE_MAX_LEN)
 
 #include <algorithm>
 #include <cmath>
@@ -27,6 +28,7 @@ typedef uint32_t u32;
 typedef uint64_t u64;
 typedef int64_t i64;
 const u32 NONE = 0xFFFFFFFFu;
+const u64 RATE_MAX_LEN = AXC_RATE_MAX_LEN;  // the rating's hyperedge length limit (include/axc.h)
 
 struct G {
     u32 n = 0, e = 0;
@@ -113,6 +115,9 @@ T touching(const G &g) {
 // of floor(w_fx(e) / |e|) (uint32, wrapping). v is dropped when
 // |in(u)| + |in(v)| - |in(u) cap in(v)| > delta, where the intersection counts hyperedges inbound
 // to u in which v is a destination. The top cnc by (score desc, id desc) with score > 0 are kept.
+// This build's one departure: hyperedges of more than RATE_MAX_LEN pins take no part in the rating
+// (their pair visits grow as |e|^2 while each pair gains only floor(w/|e|)); leaving them out of
+// the shared-inbound count only makes the delta filter stricter.
 void rating(const G &g, const std::vector<u32> &wfx, const T &t, const u32 *nsize, u32 omega,
             u32 delta, u32 cnc, u32 *pairs, u32 *scores) {
     std::vector<u32> sc(g.n, 0), cm(g.n, 0), mark(g.n, NONE);
@@ -125,6 +130,7 @@ void rating(const G &g, const std::vector<u32> &wfx, const T &t, const u32 *nsiz
             const u32 h = t.touch[j];
             const bool inb = (j - t0) < t.nin[u];
             const u64 a = g.off[h], b = g.off[h + 1];
+            if (b - a > RATE_MAX_LEN) continue;
             const u32 c = wfx[h] / (u32)(b - a);
             for (u64 k = a; k < b; ++k) {
                 const u32 v = g.pins[k];

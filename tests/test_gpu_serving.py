@@ -1,0 +1,74 @@
+"""Batching and serving: jobs of uneven size and mode run concurrently on several lanes, each with
+its own stream and device arena, and every result equals the same job partitioned alone."""
+import numpy as np
+import pytest
+
+import axoncuda_b200 as ax
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_jobs(count, seed0=200):
+    """Circuit and SNN hypergraphs of uneven size, k-way (k in 2, 8, 32) and INCC."""
+    jobs = []
+    rng = np.random.default_rng(seed0)
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1500), np.log(20000))))
+        if i % 2 == 0:
+            g = ax.gen_circuit(n, int(n * 1.1), 2, 32, 2.5, 0.9, 0.02, seed0 + i)
+        else:
+            g = ax.gen_snn(6, max(n // 6, 64), 24, 0.0, 0, 1.0, seed0 + i)
+        if i % 3 == 2:
+            p = ax.params_incc(128, 1024, 1048576, cnc=4, rfr=8)
+        else:
+            p = ax.params_kway([2, 8, 32][i % 3], 0.03, cnc=4, rfr=8)
+        jobs.append((g, p))
+    return jobs
+
+
+def test_lanes_match_solo(ctx):
+    jobs = mixed_jobs(12)
+    solo = [ctx.partition(g, p)[0] for g, p in jobs]
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(6, 8 << 30)
+        ids = [srv.submit(g, p) for g, p in jobs]
+        for (g, _), jid, s in zip(jobs, ids, solo):
+            part, st = srv.poll(jid, g.n)
+            np.testing.assert_array_equal(part, s)
+            assert st.valid == 1
+            assert st.ms_run > 0 and st.ms_queued >= 0
+            assert 0 < st.device_bytes_peak
+
+
+def test_batch_call_matches_solo(ctx):
+    jobs = mixed_jobs(8, seed0=300)
+    solo = [ctx.partition(g, p)[0] for g, p in jobs]
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(4, 8 << 30)
+        res = srv.partition_batch(jobs)
+    for (part, st), s in zip(res, solo):
+        np.testing.assert_array_equal(part, s)
+        assert st.valid == 1
+
+
+def test_budget_smaller_than_a_job_runs_it_alone(ctx):
+    """A job whose estimate exceeds the budget still runs (alone); results are unchanged."""
+    jobs = mixed_jobs(4, seed0=400)
+    solo = [ctx.partition(g, p)[0] for g, p in jobs]
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(3, 1 << 20)  # 1 MiB: nothing fits beside another job
+        ids = [srv.submit(g, p) for g, p in jobs]
+        for (g, _), jid, s in zip(jobs, ids, solo):
+            part, _ = srv.poll(jid, g.n)
+            np.testing.assert_array_equal(part, s)
+
+
+def test_configure_after_start_is_refused():
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(2, 1 << 30)
+        g, p = mixed_jobs(1)[0]
+        jid = srv.submit(g, p)
+        srv.poll(jid, g.n)
+        with pytest.raises(ax.AxcError) as e:
+            srv.serve_configure(4, 1 << 30)
+        assert e.value.code == 9  # AXC_EBUSY
