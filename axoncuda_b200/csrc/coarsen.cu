@@ -423,6 +423,17 @@ __global__ void k_remap_groups(u32 n, u32 *__restrict__ groups, const u32 *__res
 
 }  // namespace
 
+// out[0] += sum of v[0, n), out[1] = max(out[1], max of v[0, n))
+__global__ void k_sum_max(const u64 *__restrict__ v, u32 n, unsigned long long *__restrict__ out) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 x = i < n ? v[i] : 0;
+    const u64 s = warp_sum(x), m = warp_max_u64(x);
+    if ((threadIdx.x & 31) == 0) {
+        if (s) atomicAdd(&out[0], (unsigned long long)s);
+        if (m) atomicMax(&out[1], (unsigned long long)m);
+    }
+}
+
 void setup_coarsen_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_rate_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 16384 * 4));
 }
@@ -435,30 +446,37 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     RateArgs A{n, cnc, omega, delta, L.off, L.pins, L.nsrc, wfx, L.toff, L.touch, L.nin, L.nsize, pairs, scores,
                c.d_status};
     u64 *work = c.arena.alloc<u64>(n);
-    u32 *flag = c.arena.alloc<u32>(n), *list = c.arena.alloc<u32>(n);
+    u32 *flag = c.arena.alloc<u32>(n);
+    u32 *lists[4];
+    for (auto &l : lists) l = c.arena.alloc<u32>(n);
+    // device counters, read back in one round trip: [0..3] tier sizes, [4] work sum, [5] work max
+    u64 *dc = c.arena.alloc<u64>(6);
+    AXC_CUDA(cudaMemsetAsync(dc, 0, 48, c.stream));
     fill_u32(c, pairs, NONE, (u64)n * cnc);
     LAUNCH(c, k_rate_work, cdiv((u64)n * 32, 256), 256, 0, n, L.toff, L.touch, L.off, work);
-    if (pin_visits) *pin_visits = reduce_sum_u64(c, work, n);
+    LAUNCH(c, k_sum_max, cdiv(n, 256), 256, 0, work, n, (unsigned long long *)(dc + 4));
+    const u64 lim[5] = {0, RT_WARP_W, RT_BLK1_W, RT_BLK2_W, ~0ull};
+    for (int t = 0; t < 4; ++t) {
+        LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, lim[t], lim[t + 1], flag);
+        compact_indices_dn(c, flag, lists[t], n, (u32 *)(dc + t));
+    }
+    u64 h[6];
+    fetch(c, h, dc, 48);
+    if (pin_visits) *pin_visits = h[4];
+    const u32 *list = lists[0], *list2 = lists[1], *list3 = lists[2], *list4 = lists[3];
     // tier: one warp per node, table in static smem
-    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, 0ull, (u64)RT_WARP_W, flag);
-    u32 nl = compact_indices(c, flag, list, n);
+    u32 nl = (u32)h[0];
     LAUNCH(c, k_rate_warp, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
     // tier: one block per node, 4096-slot table in dynamic smem
-    u32 *list2 = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_WARP_W, (u64)RT_BLK1_W, flag);
-    nl = compact_indices(c, flag, list2, n);
+    nl = (u32)h[1];
     LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 4096 * 4, A, list2, nl, 4096u, (u32 *)nullptr);
     // tier: one block per node, 16384-slot table in dynamic smem
-    u32 *list3 = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_BLK1_W, (u64)RT_BLK2_W, flag);
-    nl = compact_indices(c, flag, list3, n);
+    nl = (u32)h[2];
     LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 16384 * 4, A, list3, nl, 16384u, (u32 *)nullptr);
     // tier: heavy nodes, tables in a global scratch slice per resident block
-    u32 *list4 = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_rate_tier, cdiv(n, 256), 256, 0, n, work, (u64)RT_BLK2_W, ~0ull, flag);
-    nl = compact_indices(c, flag, list4, n);
+    nl = (u32)h[3];
     if (nl) {
-        u64 wmax = reduce_max_u64(c, work, n);
+        u64 wmax = h[5];
         if (wmax > n) wmax = n;  // distinct neighbours never exceed the node count
         u32 cap = 64;
         while (cap < 2 * wmax && cap < (1u << 30)) cap <<= 1;

@@ -835,44 +835,76 @@ void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
 }
 
+__global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
+                               unsigned long long *__restrict__ out);
+
+// Largest gain-work bound over all nodes (out[0]) and over the block tier (out[1]).
+__global__ void k_tier_max(u32 n, const u64 *__restrict__ work, const u64 *__restrict__ toff,
+                           unsigned long long *__restrict__ out) {
+    u32 u = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 all = 0, blk = 0;
+    if (u < n) {
+        const u64 wk = work[u], deg = toff[u + 1] - toff[u];
+        all = wk;
+        if (!(wk > GN_BLOCK_W) && !(wk <= GN_WARP_W && deg <= GN_WARP_DEG)) blk = wk;
+    }
+    all = warp_max_u64(all);
+    blk = warp_max_u64(blk);
+    if ((threadIdx.x & 31) == 0) {
+        if (all) atomicMax(&out[0], (unsigned long long)all);
+        if (blk) atomicMax(&out[1], (unsigned long long)blk);
+    }
+}
+
+// Everything the level's rounds need sized on the host comes back in one round trip (a second
+// one only when some hyperedge is longer than CS_BLOCK_CAP).
 static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
     LevelPrep lp;
     const u32 e = L.e, n = L.n;
+    // [0] census block list, [1] census huge list, [2..4] node tiers, [5] gain bound,
+    // [6] largest work, [7] largest block-tier work, [8] largest hyperedge, [9] destination pins
+    u64 *dc = c.arena.alloc<u64>(10);
+    AXC_CUDA(cudaMemsetAsync(dc, 0, 80, c.stream));
     if (e) {
         u32 *flag = c.arena.alloc<u32>(e);
         lp.hblock = c.arena.alloc<u32>(e);
-        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
-        lp.n_hblock = compact_indices(c, flag, lp.hblock, e);
-        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
         lp.hhuge = c.arena.alloc<u32>(e);
-        lp.n_hhuge = compact_indices(c, flag, lp.hhuge, e);
-        if (lp.n_hhuge) {
-            lp.huge_tab = c.arena.alloc<u64>(lp.n_hhuge + 1);
-            LAUNCH(c, k_tab_sizes, cdiv(lp.n_hhuge + 1, 256), 256, 0, lp.hhuge, lp.n_hhuge, L.off, lp.huge_tab);
-            scan_excl_u64(c, lp.huge_tab, lp.huge_tab, lp.n_hhuge + 1);
-            lp.huge_tot = fetch1(c, lp.huge_tab + lp.n_hhuge);
-        }
+        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
+        compact_indices_dn(c, flag, lp.hblock, e, (u32 *)(dc + 0));
+        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
+        compact_indices_dn(c, flag, lp.hhuge, e, (u32 *)(dc + 1));
+        LAUNCH(c, k_level_bounds, cdiv(e, 256), 256, 0, e, L.off, L.nsrc, (unsigned long long *)(dc + 8));
     }
     if (n) {
         u64 *work = c.arena.alloc<u64>(n);
         lp.work = work;
-        unsigned long long *wm = c.arena.alloc<unsigned long long>(1);
-        AXC_CUDA(cudaMemsetAsync(wm, 0, 8, c.stream));
-        LAUNCH(c, k_gain_bounds, cdiv((u64)n * 32, 256), 256, 0, n, K, L.toff, L.touch, L.off, wfx, work, wm);
+        LAUNCH(c, k_gain_bounds, cdiv((u64)n * 32, 256), 256, 0, n, K, L.toff, L.touch, L.off, wfx, work,
+               (unsigned long long *)(dc + 5));
         u32 *flag = c.arena.alloc<u32>(n);
         for (u32 t = 0; t < 3; ++t) {
             lp.ntier[t] = c.arena.alloc<u32>(n);
             LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, work, L.toff, t, flag);
-            lp.ncount[t] = compact_indices(c, flag, lp.ntier[t], n);
+            compact_indices_dn(c, flag, lp.ntier[t], n, (u32 *)(dc + 2 + t));
         }
-        lp.gain_bound = fetch1(c, (const u64 *)wm);
-        if (lp.ncount[2]) lp.heavy_work_max = reduce_max_u64(c, work, n);
-        if (lp.ncount[1]) {
-            unsigned long long *bm = c.arena.alloc<unsigned long long>(1);
-            AXC_CUDA(cudaMemsetAsync(bm, 0, 8, c.stream));
-            LAUNCH(c, k_list_max, cdiv(lp.ncount[1], 256), 256, 0, lp.ntier[1], lp.ncount[1], work, bm);
-            lp.block_work_max = fetch1(c, (const u64 *)bm);
-        }
+        LAUNCH(c, k_tier_max, cdiv(n, 256), 256, 0, n, work, L.toff, (unsigned long long *)(dc + 6));
+    }
+    u64 h[10];
+    fetch(c, h, dc, 80);
+    lp.n_hblock = (u32)h[0];
+    lp.n_hhuge = (u32)h[1];
+    for (int t = 0; t < 3; ++t) lp.ncount[t] = (u32)h[2 + t];
+    lp.gain_bound = h[5];
+    lp.heavy_work_max = lp.ncount[2] ? h[6] : 0;
+    lp.block_work_max = h[7];
+    lp.max_len = h[8];
+    lp.dst_pins = h[9];
+    if (lp.n_hhuge) {
+        lp.huge_tab = c.arena.alloc<u64>(lp.n_hhuge + 1);
+        LAUNCH(c, k_tab_sizes, cdiv(lp.n_hhuge + 1, 256), 256, 0, lp.hhuge, lp.n_hhuge, L.off, lp.huge_tab);
+        scan_excl_u64(c, lp.huge_tab, lp.huge_tab, lp.n_hhuge + 1);
+        lp.huge_tot = fetch1(c, lp.huge_tab + lp.n_hhuge);
+    }
+    if (n) {
         if (c.profiling("k_gain_warp") || c.profiling("k_gain_block")) {
             unsigned long long *dg = c.arena.alloc<unsigned long long>(3);
             AXC_CUDA(cudaMemsetAsync(dg, 0, 24, c.stream));
@@ -1205,15 +1237,6 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
     if (R == 0 || L.n == 0) return 0;
     size_t m = c.arena.mark();
     LevelPrep lp = prepare_level(c, L, wfx, rp.K);
-    {
-        unsigned long long *b = c.arena.alloc<unsigned long long>(2);
-        AXC_CUDA(cudaMemsetAsync(b, 0, 16, c.stream));
-        if (L.e) LAUNCH(c, k_level_bounds, cdiv(L.e, 256), 256, 0, L.e, L.off, L.nsrc, b);
-        u64 h[2];
-        fetch(c, h, b, 16);
-        lp.max_len = h[0];
-        lp.dst_pins = h[1];
-    }
     // Graph replays need the round's scalars in device memory. Kernel-timer pairs captured in the
     // graph are read back after every replay; the bytes of the captured launches count per replay.
     const bool graph = R > 1;
