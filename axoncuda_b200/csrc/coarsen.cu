@@ -174,6 +174,56 @@ __device__ __forceinline__ u64 block_max_u64(u64 v, u64 *red) {
     return r;
 }
 
+// The top-cnc candidates of node u from its table (keys, sc, cm) of `cap` slots; block-wide.
+__device__ void rate_select(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm, u32 cap,
+                            u64 *red) {
+    u64 prev = ~0ull;
+    for (u32 r = 0; r < A.cnc; ++r) {
+        u64 best = 0;
+        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) {
+            u32 v = keys[i];
+            if (v == NONE) continue;
+            u64 k = cand_key(A, u, v, sc[i], cm[i]);
+            if (k < prev && k > best) best = k;
+        }
+        best = block_max_u64(best, red);
+        if (threadIdx.x == 0) {
+            A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
+            A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
+        }
+        prev = best;
+        if (!best) {
+            for (u32 r2 = r + 1 + threadIdx.x; r2 < A.cnc; r2 += blockDim.x) {
+                A.pairs[(u64)u * A.cnc + r2] = NONE;
+                A.scores[(u64)u * A.cnc + r2] = 0;
+            }
+            break;
+        }
+    }
+}
+
+// Heavy nodes of a level with few of them: `splits` blocks per node share the node's table in
+// global scratch (keys | sc | cm planes of nl * cap slots, cleared beforehand); block s of node
+// idx takes every splits-th group of its warps' incidence batches.
+__global__ void __launch_bounds__(RT_BLOCK) k_rate_split_acc(RateArgs A, const u32 *__restrict__ list, u32 nl,
+                                                            u32 cap, u32 splits, u32 *gtab) {
+    const u32 idx = blockIdx.x / splits, s = blockIdx.x % splits;
+    if (idx >= nl) return;
+    const u64 plane = (u64)nl * cap;
+    u32 *keys = gtab + (u64)idx * cap, *sc = keys + plane, *cm = sc + plane;
+    const u32 nw = blockDim.x >> 5;
+    rate_flat(A, list[idx], keys, sc, cm, cap - 1, 32 * (s * nw + (threadIdx.x >> 5)), 32 * nw * splits);
+}
+__global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, const u32 *__restrict__ list, u32 nl,
+                                                               u32 cap, const u32 *gtab) {
+    __shared__ u64 red[33];
+    const u32 idx = blockIdx.x;
+    if (idx >= nl) return;
+    const u64 plane = (u64)nl * cap;
+    const u32 *keys = gtab + (u64)idx * cap, *sc = keys + plane, *cm = sc + plane;
+    rate_select(A, list[idx], keys, sc, cm, cap, red);
+}
+
 // One node per block iteration; table in dynamic smem (gtab == nullptr) or in this block's
 // slice of a global scratch region.
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
@@ -209,29 +259,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
         __syncthreads();
         rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x);
         __syncthreads();
-        u64 prev = ~0ull;
-        for (u32 r = 0; r < A.cnc; ++r) {
-            u64 best = 0;
-            for (u32 i = threadIdx.x; i < cap; i += blockDim.x) {
-                u32 v = keys[i];
-                if (v == NONE) continue;
-                u64 k = cand_key(A, u, v, sc[i], cm[i]);
-                if (k < prev && k > best) best = k;
-            }
-            best = block_max_u64(best, red);
-            if (threadIdx.x == 0) {
-                A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
-                A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
-            }
-            prev = best;
-            if (!best) {
-                for (u32 r2 = r + 1 + threadIdx.x; r2 < A.cnc; r2 += blockDim.x) {
-                    A.pairs[(u64)u * A.cnc + r2] = NONE;
-                    A.scores[(u64)u * A.cnc + r2] = 0;
-                }
-                break;
-            }
-        }
+        rate_select(A, u, keys, sc, cm, cap, red);
         __syncthreads();
     }
 }
@@ -480,9 +508,20 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
         if (wmax > n) wmax = n;  // distinct neighbours never exceed the node count
         u32 cap = 64;
         while (cap < 2 * wmax && cap < (1u << 30)) cap <<= 1;
-        u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
-        u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
-        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+        const u64 split_bytes = (u64)nl * 3 * cap * 4;
+        if (nl < (u32)c.sms * 2 && split_bytes <= (512ull << 20)) {
+            // few heavy nodes: several blocks per node on a per-node table, then selection
+            const u32 splits = std::min<u32>(64, cdiv((u64)c.sms * 4, nl));
+            u32 *gtab = c.arena.alloc<u32>((u64)nl * 3 * cap);
+            AXC_CUDA(cudaMemsetAsync(gtab, 0xFF, (size_t)nl * cap * 4, c.stream));
+            AXC_CUDA(cudaMemsetAsync(gtab + (u64)nl * cap, 0, (size_t)nl * cap * 8, c.stream));
+            LAUNCH(c, k_rate_split_acc, nl * splits, RT_BLOCK, 0, A, list4, nl, cap, splits, gtab);
+            LAUNCH(c, k_rate_split_select, nl, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+        } else {
+            u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
+            u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
+            LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+        }
     }
     check_status(c);
     c.arena.release(m);

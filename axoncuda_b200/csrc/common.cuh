@@ -248,6 +248,8 @@ void scan_incl_i64(Ctx &c, const i64 *in, i64 *out, u64 n);
 // Tile state of the single-pass scans (made by axc_create, freed by axc_destroy).
 void scan_state_create(Ctx &c, u32 cap_tiles);
 void scan_state_destroy(Ctx &c);
+// Kernel attributes of the primitives (shared memory opt-in); once per device.
+void setup_prim_kernels();
 // u32 counts -> u64 exclusive offsets with out[n] = total (out has n+1 entries)
 void offsets_from_counts(Ctx &c, const u32 *counts, u64 *out, u64 n);
 // Stable LSD radix sort of (key, value) pairs by the low `bits` bits of key. In place: on

@@ -308,6 +308,7 @@ int axc_create(int device, size_t arena_bytes, axc_ctx **out) {
         AXC_CUDA(cudaMemset(c.d_status, 0, 256));
         AXC_CUDA(cudaHostAlloc((void **)&c.h_pinned, 4096, cudaHostAllocDefault));
         setup_construct_kernels();
+        setup_prim_kernels();
         setup_coarsen_kernels(c);
         setup_refine_kernels(c);
         scan_state_create(c, 1u << 18);  // single-pass scans of up to 2^29 elements
