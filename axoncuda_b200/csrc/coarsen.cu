@@ -115,6 +115,38 @@ __device__ __forceinline__ u64 cand_key(const RateArgs &A, u32 u, u32 v, u32 s, 
     return ((u64)score << 32) | v;
 }
 
+// Per-thread top-cnc candidate keys of the table slots first, first + step, ... (keys are unique:
+// the low word is the neighbour id; 0 is empty). One pass, so each neighbour's size and inbound
+// count are read once.
+__device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm,
+                                           u32 cap, u32 first, u32 step, u64 (&top)[AXC_MAX_CANDIDATES]) {
+#pragma unroll
+    for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i) top[i] = 0;
+    const u32 cnc = A.cnc;
+    u64 floor = 0;  // the list's last entry: a key must beat it to enter
+    for (u32 s = first; s < cap; s += step) {
+        const u32 v = keys[s];
+        if (v == NONE) continue;
+        u64 k = cand_key(A, u, v, sc[s], cm[s]);
+        if (k <= floor) continue;
+#pragma unroll
+        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
+            if ((u32)i < cnc && k > top[i]) {
+                const u64 t = top[i];
+                top[i] = k;
+                k = t;
+            }
+#pragma unroll
+        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
+            if ((u32)i + 1 == cnc) floor = top[i];
+    }
+}
+__device__ __forceinline__ void top_pop(u64 (&top)[AXC_MAX_CANDIDATES]) {
+#pragma unroll
+    for (int i = 0; i + 1 < (int)AXC_MAX_CANDIDATES; ++i) top[i] = top[i + 1];
+    top[AXC_MAX_CANDIDATES - 1] = 0;
+}
+
 __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u32 *__restrict__ list, u32 nlist) {
     __shared__ u32 tk[RT_WARPS][2 * RT_WARP_W], ts[RT_WARPS][2 * RT_WARP_W], tc[RT_WARPS][2 * RT_WARP_W];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -134,28 +166,15 @@ __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u
     __syncwarp();
     rate_flat(A, u, keys, sc, cm, cap - 1, 0, 32);
     __syncwarp();
-    u64 prev = ~0ull;
+    u64 top[AXC_MAX_CANDIDATES];
+    top_collect(A, u, keys, sc, cm, cap, lane, 32, top);
     for (u32 r = 0; r < A.cnc; ++r) {
-        u64 best = 0;
-        for (u32 i = lane; i < cap; i += 32) {
-            u32 v = keys[i];
-            if (v == NONE) continue;
-            u64 k = cand_key(A, u, v, sc[i], cm[i]);
-            if (k < prev && k > best) best = k;
-        }
-        best = warp_max_u64(best);
+        const u64 best = warp_max_u64(top[0]);
         if (lane == 0) {
             A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
             A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
         }
-        prev = best ? best : 0;
-        if (!best) {
-            for (u32 r2 = r + 1 + lane; r2 < A.cnc; r2 += 32) {
-                A.pairs[(u64)u * A.cnc + r2] = NONE;
-                A.scores[(u64)u * A.cnc + r2] = 0;
-            }
-            break;
-        }
+        if (best && top[0] == best) top_pop(top);
     }
 }
 
@@ -177,28 +196,15 @@ __device__ __forceinline__ u64 block_max_u64(u64 v, u64 *red) {
 // The top-cnc candidates of node u from its table (keys, sc, cm) of `cap` slots; block-wide.
 __device__ void rate_select(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm, u32 cap,
                             u64 *red) {
-    u64 prev = ~0ull;
+    u64 top[AXC_MAX_CANDIDATES];
+    top_collect(A, u, keys, sc, cm, cap, threadIdx.x, blockDim.x, top);
     for (u32 r = 0; r < A.cnc; ++r) {
-        u64 best = 0;
-        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) {
-            u32 v = keys[i];
-            if (v == NONE) continue;
-            u64 k = cand_key(A, u, v, sc[i], cm[i]);
-            if (k < prev && k > best) best = k;
-        }
-        best = block_max_u64(best, red);
+        const u64 best = block_max_u64(top[0], red);
         if (threadIdx.x == 0) {
             A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
             A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
         }
-        prev = best;
-        if (!best) {
-            for (u32 r2 = r + 1 + threadIdx.x; r2 < A.cnc; r2 += blockDim.x) {
-                A.pairs[(u64)u * A.cnc + r2] = NONE;
-                A.scores[(u64)u * A.cnc + r2] = 0;
-            }
-            break;
-        }
+        if (best && top[0] == best) top_pop(top);
     }
 }
 
@@ -497,10 +503,19 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     LAUNCH(c, k_rate_warp, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
     // tier: one block per node, 4096-slot table in dynamic smem
     nl = (u32)h[1];
-    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 4096 * 4, A, list2, nl, 4096u, (u32 *)nullptr);
+    // shared tables sized by the largest node table the tier can need (distinct neighbours never
+    // exceed min(work, n)), so smaller tables fit more blocks per SM
+    const u64 wcap = std::min<u64>(h[5], n);
+    auto tier_cap = [&](u64 hi, u32 cap_hi) {
+        u32 cap = 64;
+        while (cap < 2 * std::min<u64>(wcap, hi) && cap < cap_hi) cap <<= 1;
+        return cap;
+    };
+    const u32 cap1 = tier_cap(RT_BLK1_W, 4096u), cap2 = tier_cap(RT_BLK2_W, 16384u);
+    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * cap1 * 4, A, list2, nl, cap1, (u32 *)nullptr);
     // tier: one block per node, 16384-slot table in dynamic smem
     nl = (u32)h[2];
-    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * 16384 * 4, A, list3, nl, 16384u, (u32 *)nullptr);
+    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * cap2 * 4, A, list3, nl, cap2, (u32 *)nullptr);
     // tier: heavy nodes, tables in a global scratch slice per resident block
     nl = (u32)h[3];
     if (nl) {
