@@ -675,18 +675,6 @@ __global__ void k_gather_by_dn(const u32 *__restrict__ src, const u32 *__restric
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < *dn) dst[i] = src[idx[i]];
 }
-__global__ void k_seg_heads(const u32 *__restrict__ a, const u32 *__restrict__ b, const u32 *__restrict__ dn, u64 nmax,
-                            u32 *__restrict__ head) {
-    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nmax) return;
-    if (i >= *dn) { head[i] = 0; return; }
-    head[i] = (i == 0 || a[i] != a[i - 1] || (b && b[i] != b[i - 1])) ? 1u : 0u;
-}
-__global__ void k_seg_start(const u32 *__restrict__ head, const u32 *__restrict__ sid, const u32 *__restrict__ dn,
-                            u32 *__restrict__ start) {
-    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < *dn && head[i]) start[sid[i]] = (u32)i;
-}
 __global__ void k_clamp_count(u32 *__restrict__ cnt, u64 cap) {
     if (*cnt > cap) *cnt = (u32)cap;
 }
@@ -716,13 +704,13 @@ __global__ void k_trans_perm(const u32 *__restrict__ perm, const u32 *__restrict
 // partition exceed delta adds +1 at its rank, one that brings it back adds -1. The first event of a
 // partition assumes it started valid (kernels/refinement.cu:632-651).
 __global__ void k_trans_flags(const u32 *__restrict__ sp, const u32 *__restrict__ sr, const i64 *__restrict__ sd,
-                              const i64 *__restrict__ E, const u32 *__restrict__ head, const u32 *__restrict__ sid,
-                              const u32 *__restrict__ start, const u32 *__restrict__ dT, const u64 *__restrict__ pinb,
+                              const i64 *__restrict__ E, const u32 *__restrict__ dT, const u64 *__restrict__ pinb,
                               u64 delta, unsigned long long *__restrict__ Vi) {
     u32 j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= *dT) return;
+    const u32 nt = *dT;
+    if (j >= nt) return;
     const u32 p = sp[j];
-    const u32 st = start[sid[j] + head[j] - 1];
+    const u32 st = lower_bound_u32(sp, nt, p);  // the partition's first transition (sp is sorted)
     const i64 before = (i64)pinb[p] + (E[j] - E[st]);
     const i64 after = before + sd[j];
     const bool was_bad = (j != st) && before > (i64)delta;
@@ -763,13 +751,20 @@ __device__ __forceinline__ Best warp_best_prefix(Best b) {
 }
 // best_better is a strict total order (ties end on the rank), so the tree reduction picks the
 // same prefix as a sequential scan would.
-__global__ void k_best(const i64 *__restrict__ G, const i64 *__restrict__ Vs, const i64 *__restrict__ Vi,
-                       const u32 *__restrict__ dM, Best *__restrict__ out) {
+// pre = inclusive scan of [gain deltas | size-violation deltas | inbound-violation deltas] by rank,
+// each n long: the prefix of segment s at rank r is pre[s*n + r] - pre[s*n - 1].
+__device__ __forceinline__ i64 seg_prefix(const i64 *pre, u32 n, u32 s, u32 r) {
+    const u64 base = (u64)s * n;
+    return pre[base + r] - (s ? pre[base - 1] : 0);
+}
+__global__ void k_best(const i64 *__restrict__ pre, u32 n, int has_vi, const u32 *__restrict__ dM,
+                       Best *__restrict__ out) {
     __shared__ Best sh[32];
     Best b{0, 0, 0, 0xFFFFFFFFu};
     const u32 M = *dM;
     for (u32 r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
-        Best c{Vi ? (Vi[r] == 0 ? 1u : 0u) : 1u, Vs[r], G[r], r};
+        const u32 ok = has_vi ? (seg_prefix(pre, n, 2, r) == 0 ? 1u : 0u) : 1u;
+        Best c{ok, seg_prefix(pre, n, 1, r), seg_prefix(pre, n, 0, r), r};
         b = best_pick(b, c);
     }
     b = warp_best_prefix(b);
@@ -781,13 +776,13 @@ __global__ void k_best(const i64 *__restrict__ G, const i64 *__restrict__ Vs, co
         if (threadIdx.x == 0) out[blockIdx.x] = x;
     }
 }
-__global__ void k_best_final(const Best *__restrict__ in, u32 nb, const i64 *__restrict__ Vi, Best *__restrict__ out,
-                             u32 *__restrict__ apply) {
+__global__ void k_best_final(const Best *__restrict__ in, u32 nb, const i64 *__restrict__ pre, u32 n, int has_vi,
+                             Best *__restrict__ out, u32 *__restrict__ apply) {
     Best x = in[0];
     for (u32 i = 1; i < nb; ++i)
         if (in[i].r != 0xFFFFFFFFu && (x.r == 0xFFFFFFFFu || best_better(in[i], x))) x = in[i];
     *out = x;
-    const i64 vi = (Vi && x.r != 0xFFFFFFFFu) ? Vi[x.r] : 0;
+    const i64 vi = (has_vi && x.r != 0xFFFFFFFFu) ? seg_prefix(pre, n, 2, x.r) : 0;
     *apply = (x.r != 0xFFFFFFFFu && x.vs <= 0 && vi <= 0 && x.g >= 0) ? 1u : 0u;
 }
 __global__ void k_apply(const u32 *__restrict__ mv, const u32 *__restrict__ target, const Best *__restrict__ best,
@@ -1098,12 +1093,13 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         c.arena.release(m1);
     }
     // prefix gains in rank order
-    i64 *G = c.arena.alloc<i64>(n), *Gx = c.arena.alloc<i64>(n);
+    // per-rank deltas of the cascaded gain, the size violations and the inbound violations, in
+    // one buffer [G | Vs | Vi] so one inclusive scan makes all three prefix sums
+    i64 *raw = c.arena.alloc<i64>(3 * (u64)n), *pre = c.arena.alloc<i64>(3 * (u64)n);
+    i64 *Gx = raw, *Vs = raw + n, *Vi = raw + 2 * (u64)n;
     LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);
-    scan_incl_i64(c, Gx, G, n);
+    AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)n * 16, c.stream));  // Vs and Vi
     // size validity
-    i64 *Vs = c.arena.alloc<i64>(n);
-    AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)n * 8, c.stream));
     {
         size_t m1 = c.arena.mark();
         const u32 nemax = 2 * n;
@@ -1118,15 +1114,9 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
                (unsigned long long *)Vs);
         c.arena.release(m1);
     }
-    i64 *Vsx = c.arena.alloc<i64>(n);
-    scan_incl_i64(c, Vs, Vsx, n);
-    Vs = Vsx;
     // inbound validity (INCC only): the transitions ordered by (partition, rank), the running
     // inbound-set size of each partition along them
-    i64 *Vi = nullptr;
     if (track) {
-        Vi = c.arena.alloc<i64>(n);
-        AXC_CUDA(cudaMemsetAsync(Vi, 0, (size_t)n * 8, c.stream));
         size_t m1 = c.arena.mark();
         const u64 nt = tcap;
         const u32 rb = bits_for(n ? n - 1 : 0), pb = bits_for(rp.K ? rp.K - 1 : 0);
@@ -1145,22 +1135,16 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         i64 *sd = c.arena.alloc<i64>(nt), *E2 = c.arena.alloc<i64>(nt);
         LAUNCH(c, k_trans_perm, cdiv(nt, 256), 256, 0, perm, dT, nt, tp, tr, tdv, sp, sr, sd);
         scan_excl_i64(c, sd, E2, nt);
-        u32 *h2 = c.arena.alloc<u32>(nt), *sid2 = c.arena.alloc<u32>(nt), *st2 = c.arena.alloc<u32>(nt);
-        LAUNCH(c, k_seg_heads, cdiv(nt, 256), 256, 0, sp, (const u32 *)nullptr, dT, nt, h2);
-        scan_excl_u32(c, h2, sid2, nt);
-        LAUNCH(c, k_seg_start, cdiv(nt, 256), 256, 0, h2, sid2, dT, st2);
-        LAUNCH(c, k_trans_flags, cdiv(nt, 256), 256, 0, sp, sr, sd, E2, h2, sid2, st2, dT, pinb, (u64)rp.delta,
+        LAUNCH(c, k_trans_flags, cdiv(nt, 256), 256, 0, sp, sr, sd, E2, dT, pinb, (u64)rp.delta,
                (unsigned long long *)Vi);
         c.arena.release(m1);
-        i64 *Vix = c.arena.alloc<i64>(n);
-        scan_incl_i64(c, Vi, Vix, n);
-        Vi = Vix;
     }
+    scan_incl_i64(c, raw, pre, 3 * (u64)n);
     // best prefix and apply
     const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
     Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
-    LAUNCH(c, k_best, nbk, 256, 0, G, Vs, Vi, dM, bb + 1);
-    LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, Vi, bb, apply);
+    LAUNCH(c, k_best, nbk, 256, 0, pre, n, track ? 1 : 0, dM, bb + 1);
+    LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, pre, n, track ? 1 : 0, bb, apply);
     LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
     c.arena.release(keep);
     return apply;
