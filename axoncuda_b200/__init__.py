@@ -20,6 +20,7 @@ MODE_INCC = 0
 MODE_KWAY = 1
 MAX_CANDIDATES = 16
 FIXED_POINT_SCALE = 262144
+RATE_MAX_LEN = 128  # AXC_RATE_MAX_LEN: longer hyperedges take no part in the rating
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error", 4: "I/O error",

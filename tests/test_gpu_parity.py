@@ -98,6 +98,31 @@ def test_rating_full_size(ctx, wl):
     np.testing.assert_array_equal(scores, o_scores)
 
 
+def long_and_short_snn():
+    """Lognormal fan-out SNN: hyperedges on both sides of the rating's length limit (128 pins)."""
+    return ax.gen_snn(5, 600, 100, 0.9, 400, 0.7, 21)
+
+
+def test_rating_length_limit_matches_oracle(ctx):
+    g = dedup(long_and_short_snn())
+    lens = np.diff(g.off)
+    assert (lens > ax.RATE_MAX_LEN).any() and (lens <= ax.RATE_MAX_LEN).any()
+    ns = np.ones(g.n, np.uint32)
+    pairs, scores = ctx.stage_rating(g, ns, 64, 4096, 4)
+    o_pairs, o_scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 64, 4096, 4)
+    np.testing.assert_array_equal(pairs, o_pairs)
+    np.testing.assert_array_equal(scores, o_scores)
+
+
+def test_partition_with_long_hyperedges_matches_oracle(ctx):
+    g = long_and_short_snn()
+    p = ax.params_incc(64, 4096, 1048576, cnc=4, rfr=8)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1
+
+
 @pytest.mark.parametrize("name,cnc", [("snn_4x64.snn", 4), ("circ_2k.hgr", 8), ("snn_5x40_ln.snn", 2)])
 def test_matching_matches_oracle(ctx, name, cnc):
     g = dedup(golden(name))

@@ -90,6 +90,20 @@ def test_rating_is_symmetric():
     assert seen > 0
 
 
+@pytest.mark.parametrize("length,rated", [(128, True), (129, False)])
+def test_rating_skips_hyperedges_over_the_length_limit(length, rated):
+    """Hyperedges of more than 128 pins (AXC_RATE_MAX_LEN) take no part in the rating: with such a
+    hyperedge alone no node has a candidate; at exactly 128 pins every node has some."""
+    n = length
+    off = np.array([0, length], np.uint64)
+    pins = np.arange(length, dtype=np.uint32)
+    nsrc = np.array([1], np.uint32)
+    w = O.wfx(np.ones(1, np.float32))
+    pairs, _ = O.rating(n, off, pins, nsrc, w, np.ones(n, np.uint32), 1 << 20, 1 << 20, 4)
+    has = (pairs.reshape(n, 4)[:, 0] != O.NONE)
+    assert has.all() if rated else not has.any()
+
+
 @pytest.mark.parametrize("name", ["snn_4x64.snn", "circ_2k.hgr", "snn_5x40_ln.snn"])
 def test_oracle_partitioner_valid_and_deterministic(name):
     r = load(name)
