@@ -311,7 +311,8 @@ constexpr u32 GN_WARP_W = 128;
 constexpr u32 GN_WARPS = 4;
 constexpr u32 GN_BLOCK = 256;
 constexpr u32 GN_BLOCK_W = 4096;
-constexpr u32 GN_WARP_DEG = 256;  // incidences one warp takes; more go to a block
+constexpr u32 GN_WARP_DEG = 256;      // incidences one warp takes; more go to a block
+constexpr u32 GN_SMALL_LEVEL = 1024;  // levels with at most this many nodes use blocks only
 
 __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const u32 *__restrict__ list, u32 nl,
                                                              const u64 *__restrict__ work) {
@@ -422,14 +423,18 @@ __global__ void k_list_max(const u32 *__restrict__ list, u32 nl, const u64 *__re
     if ((threadIdx.x & 31) == 0 && m) atomicMax(out, (unsigned long long)m);
 }
 // Gain tiers: 0 = one warp (small table, at most GN_WARP_DEG incidences), 1 = one block with the
-// table in shared memory, 2 = one block with the table in global scratch.
+// table in shared memory, 2 = one block with the table in global scratch. Levels of at most
+// GN_SMALL_LEVEL nodes use no warp tier: their few nodes carry long census chains, which a block
+// splits over its warps while the rest of the GPU would idle anyway.
+__device__ __forceinline__ u32 gain_tier(u32 n, u64 wk, u64 deg) {
+    if (wk > GN_BLOCK_W) return 2u;
+    return (n > GN_SMALL_LEVEL && wk <= GN_WARP_W && deg <= GN_WARP_DEG) ? 0u : 1u;
+}
 __global__ void k_tier(u32 n, const u64 *__restrict__ work, const u64 *__restrict__ toff, u32 tier,
                        u32 *__restrict__ flag) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
-    const u64 wk = work[u], deg = toff[u + 1] - toff[u];
-    const u32 t = wk > GN_BLOCK_W ? 2u : ((wk <= GN_WARP_W && deg <= GN_WARP_DEG) ? 0u : 1u);
-    flag[u] = t == tier ? 1u : 0u;
+    flag[u] = gain_tier(n, work[u], toff[u + 1] - toff[u]) == tier ? 1u : 0u;
 }
 
 // ------------------------------------------------------------------ ranking
@@ -841,7 +846,7 @@ __global__ void k_tier_max(u32 n, const u64 *__restrict__ work, const u64 *__res
     if (u < n) {
         const u64 wk = work[u], deg = toff[u + 1] - toff[u];
         all = wk;
-        if (!(wk > GN_BLOCK_W) && !(wk <= GN_WARP_W && deg <= GN_WARP_DEG)) blk = wk;
+        if (gain_tier(n, wk, deg) == 1u) blk = wk;
     }
     all = warp_max_u64(all);
     blk = warp_max_u64(blk);
