@@ -457,6 +457,14 @@ __global__ void k_remap_groups(u32 n, u32 *__restrict__ groups, const u32 *__res
 
 }  // namespace
 
+// out += sum of v[list[i]] over i < nl
+__global__ void k_list_sum(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ v,
+                           unsigned long long *__restrict__ out) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 s = warp_sum(i < nl ? v[list[i]] : (u64)0);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, (unsigned long long)s);
+}
+
 // out[0] += sum of v[0, n), out[1] = max(out[1], max of v[0, n))
 __global__ void k_sum_max(const u64 *__restrict__ v, u32 n, unsigned long long *__restrict__ out) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -498,6 +506,20 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     fetch(c, h, dc, 48);
     if (pin_visits) *pin_visits = h[4];
     const u32 *list = lists[0], *list2 = lists[1], *list3 = lists[2], *list4 = lists[3];
+    // Kernel timer: algorithmic bytes of the block tiers, 4 per pin visit (the pin id) and 8 per
+    // candidate slot written (pair and score), per launch.
+    u64 tier_visits[3] = {0, 0, 0};
+    if (c.profiling("k_rate_block")) {
+        u64 *dv = c.arena.alloc<u64>(3);
+        AXC_CUDA(cudaMemsetAsync(dv, 0, 24, c.stream));
+        for (int t = 0; t < 3; ++t)
+            if (h[1 + t])
+                LAUNCH(c, k_list_sum, cdiv(h[1 + t], 256), 256, 0, lists[1 + t], (u32)h[1 + t], work,
+                       (unsigned long long *)(dv + t));
+        fetch(c, tier_visits, dv, 24);
+        for (int t = 0; t < 2; ++t)  // the heavy tier counts below, if it runs on k_rate_block
+            if (h[1 + t]) c.prof_bytes += 4 * tier_visits[t] + 8ull * cnc * h[1 + t];
+    }
     // tier: one warp per node, table in static smem
     u32 nl = (u32)h[0];
     LAUNCH(c, k_rate_warp, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
@@ -535,6 +557,7 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
         } else {
             u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
             u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
+            if (c.profiling("k_rate_block")) c.prof_bytes += 4 * tier_visits[2] + 8ull * cnc * nl;
             LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab);
         }
     }
