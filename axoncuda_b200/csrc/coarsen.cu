@@ -24,6 +24,7 @@ __host__ __device__ __forceinline__ u32 rated_len(u64 len) { return len <= AXC_R
 constexpr u32 RT_WARP_W = 256;     // work (incident pins) handled by one warp
 constexpr u32 RT_BLK1_W = 2048;    // block tier 1: table 4096 slots (48 KiB)
 constexpr u32 RT_BLK2_W = 8192;    // block tier 2: table 16384 slots (192 KiB)
+constexpr u32 RT_TRY = 2048;       // first-try table of the block tiers (24 KiB)
 constexpr u32 RT_WARPS = 4;
 constexpr u32 RT_BLOCK = 256;
 
@@ -60,8 +61,25 @@ struct RateArgs {
 // calling warp takes u's incidences in batches of 32 starting at `first`, every `stride` entries.
 // A batch's hyperedge metadata loads in parallel, then its pins are flattened across the lanes
 // (each lane finds its pin's hyperedge by a 5-step search over the prefix of the batch's lengths).
+// With `ndist` set, the table is a first try: distinct keys are counted there, and once they pass
+// `limit` the node stops (the caller retries it with a larger table).
+__device__ __forceinline__ u32 hash_insert_fresh(u32 *keys, u32 mask, u32 key, bool &fresh) {
+    u32 h = hslot(key, mask);
+    for (u32 probes = 0; probes <= mask; ++probes) {
+        const u32 k = keys[h];
+        if (k == key) return h;
+        if (k == NONE) {
+            const u32 prev = atomicCAS(&keys[h], NONE, key);
+            if (prev == NONE) { fresh = true; return h; }
+            if (prev == key) return h;
+        }
+        h = (h + 1) & mask;
+    }
+    return NONE;
+}
+
 __device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 first,
-                          u32 stride) {
+                          u32 stride, u32 *ndist = nullptr, u32 limit = 0) {
     const u32 lane = threadIdx.x & 31u;
     const u64 t0 = A.toff[u];
     const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
@@ -99,8 +117,17 @@ __device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm,
             const u32 i = f - eo;  // position inside the owner hyperedge
             const u32 v = A.pins[ao + i];
             if (v == u) continue;
-            const u32 slot = hash_find_or_insert(keys, mask, v);
-            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            u32 slot;
+            if (ndist) {  // bounded table: count distinct keys, give up past `limit`
+                if (*(volatile u32 *)ndist > limit) continue;
+                bool fresh = false;
+                slot = hash_insert_fresh(keys, mask, v, fresh);
+                if (fresh && atomicAdd(ndist, 1u) + 1 > limit) continue;
+                if (slot == NONE) { atomicExch(ndist, limit + 1); continue; }
+            } else {
+                slot = hash_find_or_insert(keys, mask, v);
+                if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            }
             atomicAdd(&sc[slot], cc);
             if (ib && i >= ss) atomicAdd(&cm[slot], 1u);
         }
@@ -232,16 +259,22 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, cons
 
 // One node per block iteration; table in dynamic smem (gtab == nullptr) or in this block's
 // slice of a global scratch region.
+// With `retry` set the launch is a first try on tables smaller than the nodes' work bounds: a node
+// whose distinct neighbours pass half of its table stops and is appended to retry / *d_retry.
+// With `d_nl` set the list length is read from device memory (at most nlist).
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
-                                                        u32 cap_max, u32 *gtab) {
+                                                        u32 cap_max, u32 *gtab, const u32 *__restrict__ d_nl,
+                                                        u32 *__restrict__ retry, u32 *__restrict__ d_retry) {
     extern __shared__ u32 dyn[];
     __shared__ u64 red[33];
+    __shared__ u32 ndist;
     u32 *keys, *sc, *cm;
     if (gtab) {
         keys = gtab + (u64)blockIdx.x * 3 * cap_max;
     } else {
         keys = dyn;
     }
+    if (d_nl) nlist = min(nlist, *d_nl);
     for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
         const u32 u = list[idx];
         // table size from the node's work bound, capped by the node count
@@ -262,10 +295,17 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
         sc = keys + cap;
         cm = sc + cap;
         for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
+        if (threadIdx.x == 0) ndist = 0;
         __syncthreads();
-        rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x);
+        const u32 limit = cap / 2;
+        rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x, retry ? &ndist : nullptr,
+                  limit);
         __syncthreads();
-        rate_select(A, u, keys, sc, cm, cap, red);
+        if (retry && ndist > limit) {  // table too small: the retry launch redoes this node
+            if (threadIdx.x == 0) retry[atomicAdd(d_retry, 1u)] = u;
+        } else {
+            rate_select(A, u, keys, sc, cm, cap, red);
+        }
         __syncthreads();
     }
 }
@@ -534,10 +574,28 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
         return cap;
     };
     const u32 cap1 = tier_cap(RT_BLK1_W, 4096u), cap2 = tier_cap(RT_BLK2_W, 16384u);
-    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * cap1 * 4, A, list2, nl, cap1, (u32 *)nullptr);
-    // tier: one block per node, 16384-slot table in dynamic smem
+    // Nodes' work bounds count pins with multiplicity; their distinct neighbours are usually far
+    // fewer. A first launch tries RT_TRY-slot tables (more blocks per SM); nodes that outgrow
+    // theirs are redone by a second launch with the tier's full tables.
+    u32 *retry = c.arena.alloc<u32>(n), *d_retry = (u32 *)(dc + 4);  // dc[4] was read already
+    auto block_tier = [&](const u32 *lst, u32 cnt, u32 cap_full) {
+        if (!cnt) return;
+        if (cap_full <= RT_TRY) {
+            LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * cap_full * 4, A, lst, cnt, cap_full, (u32 *)nullptr,
+                   (const u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
+            return;
+        }
+        AXC_CUDA(cudaMemsetAsync(d_retry, 0, 4, c.stream));
+        LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * RT_TRY * 4, A, lst, cnt, RT_TRY, (u32 *)nullptr,
+               (const u32 *)nullptr, retry, d_retry);
+        const u32 grid = std::min<u32>(cnt, (u32)c.sms * 2);
+        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 3 * cap_full * 4, A, (const u32 *)retry, cnt, cap_full,
+               (u32 *)nullptr, (const u32 *)d_retry, (u32 *)nullptr, (u32 *)nullptr);
+    };
+    block_tier(list2, nl, cap1);
+    // tier: one block per node, up to 16384-slot table in dynamic smem
     nl = (u32)h[2];
-    LAUNCH(c, k_rate_block, nl, RT_BLOCK, 3 * cap2 * 4, A, list3, nl, cap2, (u32 *)nullptr);
+    block_tier(list3, nl, cap2);
     // tier: heavy nodes, tables in a global scratch slice per resident block
     nl = (u32)h[3];
     if (nl) {
@@ -558,7 +616,8 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
             u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
             u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
             if (c.profiling("k_rate_block")) c.prof_bytes += 4 * tier_visits[2] + 8ull * cnc * nl;
-            LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+            LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab, (const u32 *)nullptr, (u32 *)nullptr,
+                   (u32 *)nullptr);
         }
     }
     check_status(c);
