@@ -55,6 +55,7 @@ struct RateArgs {
     const u32 *touch, *nin, *nsize;
     u32 *pairs, *scores;
     u32 *status;
+    const u64 *work;  // per node: pins visited by its rating (the table bound)
 };
 
 // Accumulate node u's neighbour scores into (keys, sc, cm) of size mask+1. Warp-cooperative: the
@@ -145,6 +146,16 @@ __device__ __forceinline__ u64 cand_key(const RateArgs &A, u32 u, u32 v, u32 s, 
 // Per-thread top-cnc candidate keys of the table slots first, first + step, ... (keys are unique:
 // the low word is the neighbour id; 0 is empty). One pass, so each neighbour's size and inbound
 // count are read once.
+// Inserts key k into the descending list top[0, cnc) (a key not above the last entry drops out).
+__device__ __forceinline__ void top_insert(u64 (&top)[AXC_MAX_CANDIDATES], u64 k, u32 cnc) {
+#pragma unroll
+    for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
+        if ((u32)i < cnc && k > top[i]) {
+            const u64 t = top[i];
+            top[i] = k;
+            k = t;
+        }
+}
 __device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm,
                                            u32 cap, u32 first, u32 step, u64 (&top)[AXC_MAX_CANDIDATES]) {
 #pragma unroll
@@ -154,15 +165,9 @@ __device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 
     for (u32 s = first; s < cap; s += step) {
         const u32 v = keys[s];
         if (v == NONE) continue;
-        u64 k = cand_key(A, u, v, sc[s], cm[s]);
+        const u64 k = cand_key(A, u, v, sc[s], cm[s]);
         if (k <= floor) continue;
-#pragma unroll
-        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
-            if ((u32)i < cnc && k > top[i]) {
-                const u64 t = top[i];
-                top[i] = k;
-                k = t;
-            }
+        top_insert(top, k, cnc);
 #pragma unroll
         for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
             if ((u32)i + 1 == cnc) floor = top[i];
@@ -181,12 +186,7 @@ __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u
     if (idx >= nlist) return;
     const u32 u = list[idx];
     u32 *keys = tk[w], *sc = ts[w], *cm = tc[w];
-    u32 W = 0;  // work bound for the table size
-    for (u64 j = A.toff[u] + lane; j < A.toff[u + 1]; j += 32) {
-        u32 h = A.touch[j];
-        W += rated_len(A.off[h + 1] - A.off[h]);
-    }
-    W = warp_sum(W);
+    const u64 W = A.work[u];  // work bound for the table size (at most RT_WARP_W in this tier)
     u32 cap = 64;
     while (cap < 2 * W) cap <<= 1;
     for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
@@ -205,34 +205,36 @@ __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u
     }
 }
 
-__device__ __forceinline__ u64 block_max_u64(u64 v, u64 *red) {
-    v = warp_max_u64(v);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        u64 x = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
-        x = warp_max_u64(x);
-        if (threadIdx.x == 0) red[32] = x;
-    }
-    __syncthreads();
-    u64 r = red[32];
-    __syncthreads();
-    return r;
-}
+constexpr u32 RT_SEL = (RT_BLOCK / 32) * AXC_MAX_CANDIDATES;  // shared slots of the block selection
 
 // The top-cnc candidates of node u from its table (keys, sc, cm) of `cap` slots; block-wide.
+// Each warp reduces its lanes' lists to its own top cnc with shuffles into red[warp * cnc ..];
+// warp 0 merges those after one barrier. red holds RT_SEL entries.
 __device__ void rate_select(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm, u32 cap,
                             u64 *red) {
+    const u32 lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5, cnc = A.cnc;
     u64 top[AXC_MAX_CANDIDATES];
     top_collect(A, u, keys, sc, cm, cap, threadIdx.x, blockDim.x, top);
-    for (u32 r = 0; r < A.cnc; ++r) {
-        const u64 best = block_max_u64(top[0], red);
-        if (threadIdx.x == 0) {
-            A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
-            A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
-        }
+    for (u32 r = 0; r < cnc; ++r) {
+        const u64 best = warp_max_u64(top[0]);
+        if (lane == 0) red[w * cnc + r] = best;
         if (best && top[0] == best) top_pop(top);
     }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i) top[i] = 0;
+        for (u32 i = lane; i < nw * cnc; i += 32) top_insert(top, red[i], cnc);
+        for (u32 r = 0; r < cnc; ++r) {
+            const u64 best = warp_max_u64(top[0]);
+            if (lane == 0) {
+                A.pairs[(u64)u * cnc + r] = best ? (u32)best : NONE;
+                A.scores[(u64)u * cnc + r] = best ? (u32)(best >> 32) : 0u;
+            }
+            if (best && top[0] == best) top_pop(top);
+        }
+    }
+    __syncthreads();  // red is reused by the block's next node
 }
 
 // Heavy nodes of a level with few of them: `splits` blocks per node share the node's table in
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_acc(RateArgs A, const u
 }
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, const u32 *__restrict__ list, u32 nl,
                                                                u32 cap, const u32 *gtab) {
-    __shared__ u64 red[33];
+    __shared__ u64 red[RT_SEL];
     const u32 idx = blockIdx.x;
     if (idx >= nl) return;
     const u64 plane = (u64)nl * cap;
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
                                                         u32 cap_max, u32 *gtab, const u32 *__restrict__ d_nl,
                                                         u32 *__restrict__ retry, u32 *__restrict__ d_retry) {
     extern __shared__ u32 dyn[];
-    __shared__ u64 red[33];
+    __shared__ u64 red[RT_SEL];
     __shared__ u32 ndist;
     u32 *keys, *sc, *cm;
     if (gtab) {
@@ -278,18 +280,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
     for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
         const u32 u = list[idx];
         // table size from the node's work bound, capped by the node count
-        __shared__ u64 Wsh;
-        if (threadIdx.x == 0) Wsh = 0;
-        __syncthreads();
-        u64 W = 0;
-        for (u64 j = A.toff[u] + threadIdx.x; j < A.toff[u + 1]; j += blockDim.x) {
-            u32 h = A.touch[j];
-            W += rated_len(A.off[h + 1] - A.off[h]);
-        }
-        W = warp_sum(W);
-        if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long *)&Wsh, (unsigned long long)W);
-        __syncthreads();
-        W = Wsh < A.n ? Wsh : A.n;
+        const u64 W = A.work[u] < A.n ? A.work[u] : A.n;
         u32 cap = 64;
         while (cap < 2 * W && cap < cap_max) cap <<= 1;
         sc = keys + cap;
@@ -525,9 +516,9 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     const u32 n = L.n;
     if (n == 0) return;
     size_t m = c.arena.mark();
-    RateArgs A{n, cnc, omega, delta, L.off, L.pins, L.nsrc, wfx, L.toff, L.touch, L.nin, L.nsize, pairs, scores,
-               c.d_status};
     u64 *work = c.arena.alloc<u64>(n);
+    RateArgs A{n, cnc, omega, delta, L.off, L.pins, L.nsrc, wfx, L.toff, L.touch, L.nin, L.nsize, pairs, scores,
+               c.d_status, work};
     u32 *flag = c.arena.alloc<u32>(n);
     u32 *lists[4];
     for (auto &l : lists) l = c.arena.alloc<u32>(n);
