@@ -177,7 +177,22 @@ struct GainArgs {
     i64 *gain;
     u32 *status;
     const u32 *dyn;  // when set: discount and round read from device memory (graph replays)
+    u32 K;           // partitions: with K <= GN_DIRECT_K the tables are indexed by partition id
 };
+
+constexpr u32 GN_DIRECT_K = 256;
+
+// Slots of a node's table: K (rounded up) when indexed by partition id, else from its work bound.
+__device__ __forceinline__ bool gain_direct(const GainArgs &A) { return A.K <= GN_DIRECT_K; }
+__device__ __forceinline__ u32 gain_cap(const GainArgs &A, u64 work, u32 cap_max) {
+    u32 cap = 32;
+    if (gain_direct(A)) {
+        while (cap < A.K) cap <<= 1;
+        return cap;
+    }
+    while (cap < 2 * work && cap < cap_max) cap <<= 1;
+    return cap;
+}
 
 // The launch's arguments with the per-round scalars resolved.
 __device__ __forceinline__ GainArgs gain_args_now(const GainArgs &A0) {
@@ -268,8 +283,14 @@ __device__ __forceinline__ void gain_flat(const GainArgs &A, u32 u, u32 p, u32 *
                 saving += leave_gain(A.encourage, wo, A.ccnt[k]);
                 continue;
             }
-            const u32 slot = hash_find_or_insert(keys, mask, q);
-            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            u32 slot;
+            if (gain_direct(A)) {  // the slot is the partition id: no probing
+                slot = q;
+                keys[q] = q;
+            } else {
+                slot = hash_find_or_insert(keys, mask, q);
+                if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+            }
             atomicAdd(&conn[slot], (unsigned long long)wo);
             if (io && A.cdcnt[k] > 0) atomicAdd(&dconn[slot], 1u);
         }
@@ -325,7 +346,7 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const 
     const u32 u = list[idx], p = A.part[u];
     u32 *keys = tk[w], *dconn = td[w];
     unsigned long long *conn = tcw[w];
-    const u32 cap = table_cap(work[u], 2 * GN_WARP_W);
+    const u32 cap = gain_cap(A, work[u], 2 * GN_WARP_W);
     for (u32 i = lane; i < cap; i += 32) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
     __syncwarp();
     i64 saving = 0, wtot = 0;
@@ -361,7 +382,7 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 
         const u32 u = list[idx], p = A.part[u];
         unsigned long long *conn;
         u32 *keys, *dconn;
-        const u32 cap = table_cap(work[u], cap_max);
+        const u32 cap = gain_cap(A, work[u], cap_max);
         if (gtab) {
             u32 *base = gtab + (u64)blockIdx.x * 4 * cap_max;  // this block's slice
             conn = (unsigned long long *)base;
@@ -802,7 +823,7 @@ GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp,
                         const u64 *psize, const u64 *pinb, u32 discount, u32 round, u32 *target, i64 *gain,
                         u32 *status) {
     GainArgs A;
-    A.n = L.n; A.omega = rp.omega; A.delta = rp.delta; A.discount = discount; A.round = round;
+    A.n = L.n; A.omega = rp.omega; A.delta = rp.delta; A.discount = discount; A.round = round; A.K = rp.K;
     A.seed = (u32)rp.seed; A.encourage = rp.encourage ? 1 : 0;
     A.off = L.off; A.lam = cs.lam; A.cpart = cs.part; A.ccnt = cs.cnt; A.cdcnt = cs.dcnt; A.wfx = wfx;
     A.toff = L.toff; A.touch = L.touch; A.nin = L.nin; A.nsize = L.nsize; A.part = part;
@@ -954,7 +975,9 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
     LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
     if (lp.ncount[1]) {
         // shared table sized by the tier's largest bound (16 B per slot)
-        const u32 cap1 = table_cap(lp.block_work_max, 2 * GN_BLOCK_W);
+        u32 cap1 = table_cap(lp.block_work_max, 2 * GN_BLOCK_W);
+        if (A.K <= GN_DIRECT_K)  // indexed by partition id: K slots (rounded up) per node
+            while (cap1 < A.K) cap1 <<= 1;
         LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, cap1 * 16, A, lp.ntier[1], lp.ncount[1], cap1, (u32 *)nullptr,
                lp.work);
     }
