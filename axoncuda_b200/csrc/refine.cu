@@ -17,6 +17,8 @@
 // Work lists that depend only on the level (hyperedge-length tiers, per-node gain-work bounds)
 // are built once per level. Inside a round every count stays in device memory; the host reads a
 // single word per round (whether moves were applied), which drives the round schedule.
+#include <cstdlib>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -497,9 +499,25 @@ struct CascadeArgs {
     u32 *dT;
     u64 tcap;
     u32 *status;
+    u32 K;  // partitions: with K <= CC_DIRECT_K the per-hyperedge tables are indexed by partition id
 };
 
 constexpr u32 MV_DST = 0x80000000u;  // mover flag in the node field: the pin is a destination
+constexpr u32 CC_DIRECT_K = 256;
+
+__device__ __forceinline__ bool cascade_direct(const CascadeArgs &A) { return A.K <= CC_DIRECT_K; }
+
+// The hyperedge's census into the table: partition -> (pins, destination pins). Block- or
+// warp-wide over threads [t0, t0 + nt); direct tables hold K slots, hashed ones `cap`.
+__device__ __forceinline__ void cascade_fill(const CascadeArgs &A, u64 a, u32 lm, u32 *tk, u32 *tc, u32 *td, u32 cap,
+                                             u32 t0, u32 nt) {
+    const bool direct = cascade_direct(A);
+    for (u32 i = t0; i < lm; i += nt) {
+        const u32 q = A.cpart[a + i];
+        const u32 s = direct ? q : hash_find_or_insert(tk, cap - 1, q);
+        if (s != NONE) { tc[s] = A.ccnt[a + i]; td[s] = A.cdcnt[a + i]; }
+    }
+}
 
 __device__ __forceinline__ void emit_transition(const CascadeArgs &A, u32 p, u32 r, int32_t d) {
     const u32 s = atomicAdd(A.dT, 1u);
@@ -509,33 +527,80 @@ __device__ __forceinline__ void emit_transition(const CascadeArgs &A, u32 p, u32
     A.tdv[s] = d;
 }
 
+// Table slots of every mover's source and target partition, sl[i] = slot(p) | slot(q) << 16,
+// gathered in parallel so the sequential sweep reads no global memory. Hashed tables insert the
+// partitions missing from the census (their counts stay zero); they need cap <= 65536.
+__device__ __forceinline__ void cascade_slots(const CascadeArgs &A, const u64 *mv, u32 *sl, u32 m, u32 *tk, u32 cap,
+                                              u32 t0, u32 nt) {
+    const bool direct = cascade_direct(A);
+    for (u32 i = t0; i < m; i += nt) {
+        const u32 v = (u32)mv[i] & ~MV_DST;
+        const u32 p = A.part[v], q = A.target[v];
+        u32 sp = p, sq = q;  // direct tables: the slot is the partition id
+        if (!direct) {
+            sp = hash_find_or_insert(tk, cap - 1, p);
+            sq = hash_find_or_insert(tk, cap - 1, q);
+            if (sp == NONE || sq == NONE) { atomicExch(A.status, DEV_HASH_FULL); sp = sq = 0; }
+        }
+        sl[i] = sp | sq << 16;
+    }
+}
+
 // Sweep the movers of one hyperedge sequentially in rank order. mv[i] = rank << 32 | dst flag |
-// node; tc / td hold the hyperedge's pins / destination pins per partition (hash slots in tk).
-__device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, u32 m, u32 *tk, u32 *tc, u32 *td,
-                              u32 mask) {
+// node; tc / td hold the hyperedge's pins / destination pins per partition (hash slots in tk,
+// or the partition id itself for direct tables). With sl the slots come precomputed from
+// cascade_slots; without it (hashed tables too large for 16-bit slots) they are looked up here.
+__device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, const u32 *sl, u32 m, u32 *tk, u32 *tc,
+                              u32 *td, u32 mask) {
     const u32 w = A.wfx[h];
+    const bool direct = cascade_direct(A);
     for (u32 i = 0; i < m; ++i) {
         const u32 lowv = (u32)mv[i], r = (u32)(mv[i] >> 32);
         const u32 v = lowv & ~MV_DST;
-        const u32 p = A.part[v], q = A.target[v];
-        const u32 sp = hash_find_or_insert(tk, mask, p), sq = hash_find_or_insert(tk, mask, q);
-        if (sp == NONE || sq == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
+        u32 sp, sq;
+        if (sl) {
+            sp = sl[i] & 0xFFFFu;
+            sq = sl[i] >> 16;
+        } else {
+            sp = A.part[v];
+            sq = A.target[v];
+            if (!direct) {
+                sp = hash_find_or_insert(tk, mask, sp);
+                sq = hash_find_or_insert(tk, mask, sq);
+                if (sp == NONE || sq == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
+            }
+        }
         const u32 cp = tc[sp], cq = tc[sq];
         const i64 d = leave_gain(A.encourage, w, cp) - (cq == 0 ? (i64)w : 0);
         atomicAdd(&A.g2[v], (unsigned long long)d);
         tc[sp] = cp - 1;
         tc[sq] = tc[sq] + 1;
         if (A.track && (lowv & MV_DST)) {
-            if (td[sp] == 1) emit_transition(A, p, r, -1);
-            if (td[sq] == 0) emit_transition(A, q, r, +1);
+            if (td[sp] == 1) emit_transition(A, direct ? sp : tk[sp], r, -1);
+            if (td[sq] == 0) emit_transition(A, direct ? sq : tk[sq], r, +1);
             td[sp] -= 1;
             td[sq] += 1;
         }
     }
 }
 
+// Table size for a hyperedge with lm census partitions and m movers: its keys are the census
+// partitions plus at most m targets, at load factor <= 1/2.
+__host__ __device__ __forceinline__ u64 cascade_cap(u64 lm, u64 m) {
+    u64 cap = 32;
+    while (cap < 2 * (lm + m)) cap <<= 1;
+    return cap;
+}
+__device__ __forceinline__ u32 cascade_cap32(u32 lm, u32 m) {
+    const u64 cap = cascade_cap(lm, m);
+    return cap > (1ull << 31) ? (1u << 31) : (u32)cap;
+}
+
+// Hyperedges with at most CC_MOV movers, one warp each (hashed tables also need at most CC_TAB
+// slots); the others are appended to `big` for the block kernel.
 __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__restrict__ nbig) {
     __shared__ u64 mvs[CC_WARPS][CC_MOV];
+    __shared__ u32 sl[CC_WARPS][CC_MOV];
     __shared__ u32 tk[CC_WARPS][CC_TAB], tc[CC_WARPS][CC_TAB], td[CC_WARPS][CC_TAB];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 h = blockIdx.x * CC_WARPS + w;
@@ -556,7 +621,9 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__rest
     }
     if (m == 0) return;
     const u32 lm = A.lam[h];
-    if (m > CC_MOV || 2 * (lm + 2 * m) > CC_TAB) {
+    const bool direct = cascade_direct(A);
+    const u32 cap = direct ? A.K : cascade_cap32(lm, m);
+    if (m > CC_MOV || cap > CC_TAB) {
         if (lane == 0) big[atomicAdd(nbig, 1u)] = h;  // handled by the block kernel
         return;
     }
@@ -573,17 +640,14 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__rest
     __syncwarp();
     for (u32 i = 0; i < CC_MOV / 32; ++i)
         if (lane + 32 * i < m) mvs[w][posv[i]] = mine[i];
-    // table of partition counts from the census
-    u32 cap = 32;
-    while (cap < 2 * (lm + 2 * m)) cap <<= 1;
+    // table of partition counts from the census, then the movers' slots
     for (u32 i = lane; i < cap; i += 32) { tk[w][i] = NONE; tc[w][i] = 0; td[w][i] = 0; }
     __syncwarp();
-    for (u32 i = lane; i < lm; i += 32) {
-        u32 s = hash_find_or_insert(tk[w], cap - 1, A.cpart[a + i]);
-        if (s != NONE) { tc[w][s] = A.ccnt[a + i]; td[w][s] = A.cdcnt[a + i]; }
-    }
+    cascade_fill(A, a, lm, tk[w], tc[w], td[w], cap, lane, 32);
     __syncwarp();
-    if (lane == 0) cascade_sweep(A, h, mvs[w], m, tk[w], tc[w], td[w], cap - 1);
+    cascade_slots(A, mvs[w], sl[w], m, tk[w], cap, lane, 32);
+    __syncwarp();
+    if (lane == 0) cascade_sweep(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], cap - 1);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -605,46 +669,89 @@ __device__ void block_bitonic_u64(u64 *buf, u32 P) {
     }
 }
 
-constexpr u32 CB_SMEM = 4096;  // movers sorted in shared memory (32 KB); larger sets sort in scratch
+constexpr u32 CB_THREADS = 128;
+constexpr u32 CB_MOV_MAX = 2048;  // movers of the block kernel, in shared memory
+constexpr u32 CB_TAB_HASH = 1024; // hashed table slots of the block kernel
 
-// Hyperedges with many movers: one block at a time per hyperedge. Movers are sorted by rank with
-// a bitonic sort, in shared memory when the hyperedge has at most CB_SMEM pins, else in this
-// block's slice of a scratch region (mv_cap entries, a power of two >= the largest hyperedge).
-__global__ void k_cascade_big(CascadeArgs A, const u32 *__restrict__ list, const u32 *__restrict__ nl, u64 *scratch_mv,
-                              u32 *scratch_tab, u64 mv_cap, u64 tab_cap) {
-    __shared__ u64 smv[CB_SMEM];
+// Gather the movers of hyperedge h (rank << 32 | dst flag | node) into mvs[0, min(m, lim)) with
+// the whole block; returns m (all of them, counted past lim). Ends with the block synchronised.
+__device__ __forceinline__ u32 cascade_gather(const CascadeArgs &A, u32 h, u64 *mvs, u32 lim, u32 *cntm) {
+    const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
+    if (threadIdx.x == 0) *cntm = 0;
+    __syncthreads();
+    for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
+        const u32 v = A.pins[k], r = A.rank[v];
+        if (r != NONE) {
+            const u32 pos = atomicAdd(cntm, 1u);
+            if (pos < lim) mvs[pos] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
+        }
+    }
+    __syncthreads();
+    const u32 m = *cntm;
+    __syncthreads();  // the count is read before the next hyperedge resets it
+    return m;
+}
+
+// Sort, tables, slots and sweep of one hyperedge whose m movers are in mvs (block-wide).
+__device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u64 *mvs, u32 *sl, u32 m, u32 *tk,
+                                                  u32 *tc, u32 *td, u32 cap) {
+    u32 P = 1;
+    while (P < m) P <<= 1;
+    for (u32 i = m + threadIdx.x; i < P; i += blockDim.x) mvs[i] = ~0ull;
+    for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tk[i] = NONE; tc[i] = 0; td[i] = 0; }
+    __syncthreads();
+    block_bitonic_u64(mvs, P);
+    cascade_fill(A, A.off[h], A.lam[h], tk, tc, td, cap, threadIdx.x, blockDim.x);
+    __syncthreads();
+    if (sl) {
+        cascade_slots(A, mvs, sl, m, tk, cap, threadIdx.x, blockDim.x);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cascade_sweep(A, h, mvs, sl, m, tk, tc, td, cap - 1);
+    __syncthreads();
+}
+
+// Hyperedges with more movers than a warp takes: one block per hyperedge, everything in shared
+// memory (dynamic: smov movers and their slots, then three tables of stab slots). Movers are
+// sorted by rank with a bitonic sort. A hyperedge with more than smov movers, or a hashed table
+// above stab slots, is appended to `huge`.
+__global__ void __launch_bounds__(CB_THREADS) k_cascade_block(CascadeArgs A, const u32 *__restrict__ list,
+                                                              const u32 *__restrict__ nl, u32 smov, u32 stab,
+                                                              u32 *__restrict__ huge, u32 *__restrict__ nhuge) {
+    extern __shared__ __align__(16) unsigned char cb_smem[];
     __shared__ u32 cntm;
-    u64 *gmv = scratch_mv + (u64)blockIdx.x * mv_cap;
+    u64 *mvs = (u64 *)cb_smem;
+    u32 *sl = (u32 *)(mvs + smov), *tk = sl + smov, *tc = tk + stab, *td = tc + stab;
+    const bool direct = cascade_direct(A);
     for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
         const u32 h = list[idx];
-        const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
-        const u32 lm = A.lam[h];
-        u64 *mvs = (b - a) <= CB_SMEM ? smv : gmv;
-        if (threadIdx.x == 0) cntm = 0;
-        __syncthreads();
-        for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
-            u32 v = A.pins[k], r = A.rank[v];
-            if (r != NONE) mvs[atomicAdd(&cntm, 1u)] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
+        const u32 m = cascade_gather(A, h, mvs, smov, &cntm);
+        const u32 cap = direct ? A.K : cascade_cap32(A.lam[h], m);
+        if (m > smov || cap > stab) {
+            if (threadIdx.x == 0) huge[atomicAdd(nhuge, 1u)] = h;
+            continue;
         }
-        __syncthreads();
-        const u32 m = cntm;
-        u32 P = 1;
-        while (P < m) P <<= 1;
-        for (u32 i = m + threadIdx.x; i < P; i += blockDim.x) mvs[i] = ~0ull;
-        __syncthreads();
-        block_bitonic_u64(mvs, P);
-        u32 cap = 32;
-        while (cap < 2 * (lm + 2 * m)) cap <<= 1;
-        u32 *tk = scratch_tab + (u64)blockIdx.x * tab_cap, *tc = tk + cap, *td = tc + cap;
-        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tk[i] = NONE; tc[i] = 0; td[i] = 0; }
-        __syncthreads();
-        for (u32 i = threadIdx.x; i < lm; i += blockDim.x) {
-            u32 s = hash_find_or_insert(tk, cap - 1, A.cpart[a + i]);
-            if (s != NONE) { tc[s] = A.ccnt[a + i]; td[s] = A.cdcnt[a + i]; }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) cascade_sweep(A, h, mvs, m, tk, tc, td, cap - 1);
-        __syncthreads();
+        cascade_block_one(A, h, mvs, sl, m, tk, tc, td, cap);
+    }
+}
+
+// The rest: one block per SM, each with its slice of scratch regions sized by the level's
+// largest hyperedge (mv_cap movers and slots, three tables of tab_cap slots).
+__global__ void __launch_bounds__(CB_THREADS) k_cascade_huge(CascadeArgs A, const u32 *__restrict__ list,
+                                                             const u32 *__restrict__ nl, u64 *scratch_mv,
+                                                             u32 *scratch_sl, u32 *scratch_tab, u64 mv_cap,
+                                                             u64 tab_cap) {
+    __shared__ u32 cntm;
+    u64 *mvs = scratch_mv + (u64)blockIdx.x * mv_cap;
+    u32 *tk = scratch_tab + (u64)blockIdx.x * 3 * tab_cap, *tc = tk + tab_cap, *td = tc + tab_cap;
+    const bool direct = cascade_direct(A);
+    for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
+        const u32 h = list[idx];
+        const u32 m = cascade_gather(A, h, mvs, (u32)mv_cap, &cntm);
+        const u32 cap = direct ? A.K : cascade_cap32(A.lam[h], m);
+        // 16-bit slots cover every direct table and hashed tables of up to 65536 slots
+        u32 *sl = (direct || cap <= 65536) ? scratch_sl + (u64)blockIdx.x * mv_cap : nullptr;
+        cascade_block_one(A, h, mvs, sl, m, tk, tc, td, cap);
     }
 }
 
@@ -850,6 +957,19 @@ struct LevelPrep {
     u64 dst_pins = 0;        // destination pins (bounds the inbound events: 2 per pin)
     u64 tier_deg[3] = {0, 0, 0};  // incidence entries of each gain tier (kernel timer only)
 };
+
+// Movers the cascade's block kernel keeps in shared memory: CB_MOV_MAX, or less when the
+// environment variable AXC_CASCADE_BLOCK_MOVERS asks for it (a power of two >= 128), which sends
+// hyperedges with more movers to the scratch kernel; the tests use it to reach that kernel on
+// small inputs. Read at each level's launch, so it applies to the next partition.
+static u32 cascade_block_movers() {
+    const char *s = std::getenv("AXC_CASCADE_BLOCK_MOVERS");
+    if (!s || !*s) return CB_MOV_MAX;
+    const unsigned long v = std::strtoul(s, nullptr, 10);
+    u32 lim = 128;
+    while ((unsigned long)lim * 2 <= v && lim < CB_MOV_MAX) lim <<= 1;
+    return lim;
+}
 
 void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_census_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 2 * CS_BLOCK_CAP * 4));
@@ -1062,10 +1182,10 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     A.dyn = dyn;
     run_gains(c, L, lp, A);
     // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
-    // [3] big cascade hyperedges
+    // [3] cascade hyperedges for the block kernel, [4] for the scratch kernel
     u32 *cnt = c.arena.alloc<u32>(8);
     AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
-    u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3;
+    u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4;
     // movers in id order, then ranked by (gain desc, id asc)
     u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n);
     LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag);
@@ -1106,18 +1226,35 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         C.part = part; C.target = target; C.g2 = g2;
         C.track = track ? 1 : 0; C.tp = tp; C.tr = tr; C.tdv = tdv; C.dT = dT; C.tcap = tcap;
         C.status = c.d_status;
+        C.K = rp.K;
+        const bool direct = rp.K <= CC_DIRECT_K;
         size_t m1 = c.arena.mark();
-        u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1);
-        if (L.e) LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
-        // scratch per resident block, sized by the level's largest hyperedge
-        u64 mv_cap = 1;
-        while (mv_cap < lp.max_len) mv_cap <<= 1;
-        u64 cap = 32;
-        while (cap < 2 * (3 * mv_cap)) cap <<= 1;
-        const u32 grid = (u32)c.sms;
-        u64 *smv = c.arena.alloc<u64>((u64)grid * mv_cap);
-        u32 *stab = c.arena.alloc<u32>((u64)grid * 3 * cap);
-        if (L.e) LAUNCH(c, k_cascade_big, grid, 256, 0, C, big, dBig, smv, stab, mv_cap, 3 * cap);
+        u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1), *huge = c.arena.alloc<u32>(L.e ? L.e : 1);
+        if (L.e) {
+            LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
+            // block kernel: shared memory sized by the level's largest hyperedge, all resident blocks
+            u32 smov = 128;
+            while (smov < lp.max_len && smov < cascade_block_movers()) smov <<= 1;
+            const u32 stab = direct ? std::max(rp.K, 32u) : CB_TAB_HASH;
+            const size_t dyn = (size_t)smov * 12 + (size_t)stab * 12;
+            int per_sm = 1;
+            AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade_block, CB_THREADS, dyn));
+            const u32 grid = (u32)c.sms * (u32)std::max(per_sm, 1);
+            LAUNCH(c, k_cascade_block, grid, CB_THREADS, dyn, C, big, dBig, smov, stab, huge, dHuge);
+            // scratch kernel, only when some hyperedge can outgrow the block kernel: one slice of
+            // movers, slots and tables per block, at most 1 GiB in all
+            u64 mv_cap = 1;
+            while (mv_cap < lp.max_len) mv_cap <<= 1;
+            const u64 tab_cap = direct ? stab : cascade_cap(lp.max_len, lp.max_len);
+            if (mv_cap > smov || tab_cap > stab) {
+                const u64 per_block = mv_cap * 12 + tab_cap * 12;
+                const u32 gh = (u32)std::max<u64>(1, std::min<u64>((u64)c.sms, (1ull << 30) / per_block));
+                u64 *smv = c.arena.alloc<u64>((u64)gh * mv_cap);
+                u32 *ssl = c.arena.alloc<u32>((u64)gh * mv_cap);
+                u32 *stb = c.arena.alloc<u32>((u64)gh * 3 * tab_cap);
+                LAUNCH(c, k_cascade_huge, gh, CB_THREADS, 0, C, huge, dHuge, smv, ssl, stb, mv_cap, tab_cap);
+            }
+        }
         c.arena.release(m1);
     }
     // prefix gains in rank order

@@ -123,6 +123,31 @@ def test_partition_with_long_hyperedges_matches_oracle(ctx):
     assert st.valid == 1
 
 
+# The refinement cascade sweeps each hyperedge's movers in rank order with one of three kernels:
+# a warp (up to 128 movers), a block with shared-memory tables, or a block on scratch memory. Its
+# tables are indexed by partition id up to 256 partitions and hashed above. The k-way case keeps
+# K = 4 (direct tables); the INCC case with omega 8 ends with more than 256 partitions (hashed).
+# AXC_CASCADE_BLOCK_MOVERS=128 sends every hyperedge with more than 128 movers to the scratch
+# kernel, which the default routing reaches only for hyperedges above 2048 pins.
+CASCADE_CASES = [ax.params_kway(4, 0.03, cnc=4, rfr=8), ax.params_incc(8, 2048, 1048576, cnc=4, rfr=8)]
+
+
+@pytest.mark.parametrize("block_movers", [None, "128"])
+@pytest.mark.parametrize("i", range(len(CASCADE_CASES)))
+def test_cascade_kernels_match_oracle(ctx, monkeypatch, i, block_movers):
+    g, p = long_and_short_snn(), CASCADE_CASES[i]
+    if block_movers is None:
+        monkeypatch.delenv("AXC_CASCADE_BLOCK_MOVERS", raising=False)
+    else:
+        monkeypatch.setenv("AXC_CASCADE_BLOCK_MOVERS", block_movers)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1
+    if p.mode == ax.MODE_INCC:
+        assert st.num_parts > 256
+
+
 @pytest.mark.parametrize("name,cnc", [("snn_4x64.snn", 4), ("circ_2k.hgr", 8), ("snn_5x40_ln.snn", 2)])
 def test_matching_matches_oracle(ctx, name, cnc):
     g = dedup(golden(name))
