@@ -64,21 +64,6 @@ struct RateArgs {
 // (each lane finds its pin's hyperedge by a 5-step search over the prefix of the batch's lengths).
 // With `ndist` set, the table is a first try: distinct keys are counted there, and once they pass
 // `limit` the node stops (the caller retries it with a larger table).
-__device__ __forceinline__ u32 hash_insert_fresh(u32 *keys, u32 mask, u32 key, bool &fresh) {
-    u32 h = hslot(key, mask);
-    for (u32 probes = 0; probes <= mask; ++probes) {
-        const u32 k = keys[h];
-        if (k == key) return h;
-        if (k == NONE) {
-            const u32 prev = atomicCAS(&keys[h], NONE, key);
-            if (prev == NONE) { fresh = true; return h; }
-            if (prev == key) return h;
-        }
-        h = (h + 1) & mask;
-    }
-    return NONE;
-}
-
 __device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 first,
                           u32 stride, u32 *ndist = nullptr, u32 limit = 0) {
     const u32 lane = threadIdx.x & 31u;

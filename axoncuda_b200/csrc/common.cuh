@@ -227,6 +227,22 @@ __device__ __forceinline__ u32 hash_find_or_insert(u32 *keys, u32 mask, u32 key)
     }
     return NONE;
 }
+// hash_find_or_insert that also reports whether this call inserted the key (`fresh`).
+__device__ __forceinline__ u32 hash_insert_fresh(u32 *keys, u32 mask, u32 key, bool &fresh) {
+    fresh = false;
+    u32 h = hslot(key, mask);
+    for (u32 probes = 0; probes <= mask; ++probes) {
+        const u32 k = keys[h];
+        if (k == key) return h;
+        if (k == NONE) {
+            const u32 prev = atomicCAS(&keys[h], NONE, key);
+            if (prev == NONE) { fresh = true; return h; }
+            if (prev == key) return h;
+        }
+        h = (h + 1) & mask;
+    }
+    return NONE;
+}
 __device__ __forceinline__ u32 hash_find(const u32 *keys, u32 mask, u32 key) {
     u32 h = hslot(key, mask);
     for (u32 probes = 0; probes <= mask; ++probes) {

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <omp.h>
 #include <string>
 #include <vector>
 
@@ -131,80 +132,151 @@ extern "C" int axc_read_axh(const char *path, axc_hgraph *out) {
 }
 
 // .hgr (hMETIS): "E V [fmt]" header, E net lines "[w] v1 v2 ...", '%' comments.
+//
+// Parsed in parallel (OpenMP): the line breaks are found per chunk of the buffer, the lines are
+// classified (blank and '%' lines are not data), and the net lines are parsed twice, once to
+// count and check each net and once, after a prefix sum over the kept nets, to write its pins.
+// The result, and which inputs fail, are those of a line-by-line reading.
+namespace {
+
+bool hgr_u64(const char *&q, const char *le, uint64_t &v) {
+    while (q < le && (*q == ' ' || *q == '\t')) ++q;
+    if (q >= le || *q < '0' || *q > '9') return false;
+    uint64_t x = 0;
+    while (q < le && *q >= '0' && *q <= '9') {
+        x = x * 10 + (uint64_t)(*q - '0');
+        if (x > 0xFFFFFFFFFFull) return false;
+        ++q;
+    }
+    v = x;
+    return true;
+}
+
+// One net line: its weight and pins (1-based ids in the file, 0-based out). Counts the pins and
+// writes them when `pins` is set. Returns false for a malformed line ("Invalid node
+// encountered", a missing weight or no node at all).
+bool hgr_net(const char *q, const char *le, bool edge_w, uint64_t V, float &w, uint64_t &cnt, uint32_t *pins) {
+    w = 1.0f;
+    if (edge_w) {
+        char tmp[64];
+        while (q < le && (*q == ' ' || *q == '\t')) ++q;
+        size_t k = 0;
+        while (q < le && *q != ' ' && *q != '\t' && k < 63) tmp[k++] = *q++;
+        tmp[k] = 0;
+        char *ep = nullptr;
+        w = std::strtof(tmp, &ep);
+        if (ep == tmp) return false;
+    }
+    cnt = 0;
+    uint64_t v;
+    while (hgr_u64(q, le, v)) {
+        if (v == 0 || v > V) return false;
+        if (pins) pins[cnt] = (uint32_t)(v - 1);
+        ++cnt;
+    }
+    return cnt > 0;
+}
+
+}  // namespace
+
 extern "C" int axc_read_hgr(const char *path, axc_hgraph *out) {
     if (!path || !out) return AXC_EINVAL;
     std::vector<char> buf;
     if (!read_file(path, buf)) return AXC_EIO;
     buf.push_back('\n');
-    const char *p = buf.data(), *end = buf.data() + buf.size();
-    // next data line: skip blank and '%' lines (hgraph.hpp:940-950)
-    auto next_line = [&](const char *&ls, const char *&le) -> bool {
-        while (p < end) {
-            const char *s = p;
-            const char *e = (const char *)std::memchr(p, '\n', (size_t)(end - p));
-            if (!e) e = end;
-            p = e + 1;
-            const char *q = s;
-            while (q < e && (*q == ' ' || *q == '\t')) ++q;
-            const char *ee = e;
-            if (ee > q && ee[-1] == '\r') --ee;
-            if (q == ee || *q == '%') continue;
-            ls = q; le = ee;
-            return true;
+    const char *base = buf.data();
+    const size_t N = buf.size();
+    // line ends ('\n' positions), found per chunk
+    const int T = std::max(1, omp_get_max_threads());
+    const size_t chunk = (N + (size_t)T - 1) / (size_t)T;
+    std::vector<size_t> ccount((size_t)T + 1, 0);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; ++t) {
+        const size_t a = std::min(N, (size_t)t * chunk), b = std::min(N, a + chunk);
+        size_t c = 0;
+        for (const char *x = base + a, *e = base + b; x < e; ++c) {
+            x = (const char *)std::memchr(x, '\n', (size_t)(e - x));
+            if (!x) break;
+            ++x;
         }
-        return false;
-    };
-    auto parse_u64 = [](const char *&q, const char *le, uint64_t &v) -> bool {
-        while (q < le && (*q == ' ' || *q == '\t')) ++q;
-        if (q >= le || *q < '0' || *q > '9') return false;
-        uint64_t x = 0;
-        while (q < le && *q >= '0' && *q <= '9') {
-            x = x * 10 + (uint64_t)(*q - '0');
-            if (x > 0xFFFFFFFFFFull) return false;
-            ++q;
+        ccount[(size_t)t + 1] = c;
+    }
+    for (int t = 0; t < T; ++t) ccount[(size_t)t + 1] += ccount[(size_t)t];
+    const size_t L = ccount[(size_t)T];
+    std::vector<size_t> lend(L);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; ++t) {
+        const size_t a = std::min(N, (size_t)t * chunk), b = std::min(N, a + chunk);
+        size_t i = ccount[(size_t)t];
+        for (const char *x = base + a, *e = base + b; x < e;) {
+            x = (const char *)std::memchr(x, '\n', (size_t)(e - x));
+            if (!x) break;
+            lend[i++] = (size_t)(x - base);
+            ++x;
         }
-        v = x;
-        return true;
-    };
-    const char *ls, *le;
-    if (!next_line(ls, le)) return AXC_EFORMAT;  // "Empty .hgr file"
+    }
+    // data lines: trimmed of leading blanks and a trailing '\r'; blank and '%' lines skipped
+    // (hgraph.hpp:940-950)
+    std::vector<uint32_t> isdata(L);
+    std::vector<size_t> lbeg(L), lfin(L);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (size_t i = 0; i < L; ++i) {
+        const size_t s0 = i ? lend[i - 1] + 1 : 0;
+        const char *q = base + s0, *e = base + lend[i];
+        while (q < e && (*q == ' ' || *q == '\t')) ++q;
+        const char *ee = e;
+        if (ee > q && ee[-1] == '\r') --ee;
+        isdata[i] = (q == ee || *q == '%') ? 0u : 1u;
+        lbeg[i] = (size_t)(q - base);
+        lfin[i] = (size_t)(ee - base);
+    }
+    std::vector<size_t> data;
+    data.reserve(L);
+    for (size_t i = 0; i < L; ++i)
+        if (isdata[i]) data.push_back(i);
+    if (data.empty()) return AXC_EFORMAT;  // "Empty .hgr file"
     uint64_t E64, V64, fmt = 0;
-    const char *q = ls;
-    if (!parse_u64(q, le, E64) || !parse_u64(q, le, V64)) return AXC_EFORMAT;
-    if (E64 > 0xFFFFFFFFull || V64 > 0xFFFFFFFFull) return AXC_EFORMAT;
-    if (!parse_u64(q, le, fmt)) fmt = 0;
+    {
+        const char *q = base + lbeg[data[0]], *le = base + lfin[data[0]];
+        if (!hgr_u64(q, le, E64) || !hgr_u64(q, le, V64)) return AXC_EFORMAT;
+        if (E64 > 0xFFFFFFFFull || V64 > 0xFFFFFFFFull) return AXC_EFORMAT;
+        if (!hgr_u64(q, le, fmt)) fmt = 0;
+    }
+    if (data.size() - 1 < E64) return AXC_EFORMAT;  // unexpected end of file
     const bool edge_w = (fmt == 1 || fmt == 11);
+    // pass 1: count and check every net; singleton nets are skipped (hgraph.hpp:989-992)
+    std::vector<uint64_t> cnt(E64 + 1, 0);
+    std::vector<float> wv(E64);
+    int bad = 0;
+#pragma omp parallel for num_threads(T) schedule(dynamic, 4096) reduction(| : bad)
+    for (int64_t i = 0; i < (int64_t)E64; ++i) {
+        const size_t l = data[(size_t)i + 1];
+        uint64_t c = 0;
+        if (!hgr_net(base + lbeg[l], base + lfin[l], edge_w, V64, wv[(size_t)i], c, nullptr)) bad |= 1;
+        cnt[(size_t)i] = c == 1 ? 0 : c;
+    }
+    if (bad) return AXC_EFORMAT;
     auto *hg = new HostGraph();
     hg->n = (uint32_t)V64;
+    std::vector<uint64_t> poff(E64 + 1, 0);
+    for (uint64_t i = 0; i < E64; ++i) poff[i + 1] = poff[i] + cnt[i];
+    hg->pins.resize(poff[E64]);
+    // pass 2: write the kept nets' pins
+#pragma omp parallel for num_threads(T) schedule(dynamic, 4096)
+    for (int64_t i = 0; i < (int64_t)E64; ++i) {
+        if (!cnt[(size_t)i]) continue;
+        const size_t l = data[(size_t)i + 1];
+        float w;
+        uint64_t c;
+        hgr_net(base + lbeg[l], base + lfin[l], edge_w, V64, w, c, hg->pins.data() + poff[(size_t)i]);
+    }
     hg->off.reserve(E64 + 1);
     hg->off.push_back(0);
-    std::vector<uint32_t> nodes;
     for (uint64_t i = 0; i < E64; ++i) {
-        if (!next_line(ls, le)) { delete hg; return AXC_EFORMAT; }  // unexpected end of file
-        q = ls;
-        float w = 1.0f;
-        if (edge_w) {
-            char tmp[64];
-            while (q < le && (*q == ' ' || *q == '\t')) ++q;
-            size_t k = 0;
-            while (q < le && *q != ' ' && *q != '\t' && k < 63) tmp[k++] = *q++;
-            tmp[k] = 0;
-            char *ep = nullptr;
-            w = std::strtof(tmp, &ep);
-            if (ep == tmp) { delete hg; return AXC_EFORMAT; }
-        }
-        nodes.clear();
-        uint64_t v;
-        while (parse_u64(q, le, v)) {
-            if (v == 0 || v > V64) { delete hg; return AXC_EFORMAT; }  // "Invalid node encountered"
-            nodes.push_back((uint32_t)(v - 1));
-        }
-        if (nodes.empty()) { delete hg; return AXC_EFORMAT; }
-        if (nodes.size() == 1) continue;  // singleton nets are skipped (hgraph.hpp:989-992)
-        hg->pins.insert(hg->pins.end(), nodes.begin(), nodes.end());
+        if (!cnt[i]) continue;
         hg->nsrc.push_back(0);
-        hg->w.push_back(w);
-        hg->off.push_back(hg->pins.size());
+        hg->w.push_back(wv[i]);
+        hg->off.push_back(poff[i + 1]);
     }
     publish(hg, out);
     return AXC_OK;

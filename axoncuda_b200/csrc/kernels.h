@@ -63,6 +63,14 @@ struct Census {
     u32 *cnt = nullptr;   // [P]
     u32 *dcnt = nullptr;  // [P]
     u32 *lam = nullptr;   // [e]
+    // Optional, for the refinement's partition-indexed gains (K <= 256): the census also adds to
+    // save[v] what each node saves by leaving its partition (needs wfx and encourage), and
+    // census_masks writes per-hyperedge bitmasks of the partitions present / with destinations.
+    i64 *save = nullptr;  // [n]
+    const u32 *wfx = nullptr;
+    int encourage = 0;
+    u32 *mask = nullptr, *dmask = nullptr;  // [e * mw]
+    u32 mw = 0;
 };
 Census build_census(Ctx &c, const DLevel &L, const u32 *part);
 void part_sizes(Ctx &c, u32 n, const u32 *part, const u32 *nsize, u64 *psize, u32 K);

@@ -29,12 +29,23 @@ constexpr u32 CS_WARP_CAP = 256;
 constexpr u32 CS_BLOCK_CAP = 4096;
 constexpr u32 CS_WARPS = 4;
 
+// What a node saves by leaving partition p of a hyperedge (weight w) where p holds c of its pins:
+// INCC (encourage) floor(w / c^2), k-way w when the node is the last pin in p.
+__device__ __forceinline__ i64 leave_gain(int encourage, u32 w, u32 c) {
+    if (encourage) return c >= 1 ? (i64)((u64)w / ((u64)c * c)) : 0;
+    return c == 1 ? (i64)w : 0;
+}
+
 // ------------------------------------------------------------------ census
 struct CensusArgs {
     const u64 *off;
     const u32 *pins, *nsrc, *part;
     u32 *cpart, *ccnt, *cdcnt, *lam;
     u32 *status;
+    // when set: every pin adds leave_gain(w, count of its partition) to its node's saving
+    unsigned long long *save;
+    const u32 *wfx;
+    int encourage;
 };
 
 // insert phase: keys = partition, mn = first position, cnt/dcnt counters
@@ -74,6 +85,8 @@ __global__ void k_census_warp(u32 e, CensusArgs A) {
             p = A.part[A.pins[k]];
             slot = hash_find(keys, cap - 1, p);
         }
+        if (A.save && slot != NONE)
+            atomicAdd(&A.save[A.pins[k]], (unsigned long long)leave_gain(A.encourage, A.wfx[h], cnt[slot]));
         bool first = slot != NONE && mn[slot] == (u32)(k - a);
         u32 bal = __ballot_sync(0xFFFFFFFFu, first);
         if (first) {
@@ -112,6 +125,8 @@ __global__ void k_census_block(const u32 *__restrict__ list, u32 nlist, CensusAr
             p = A.part[A.pins[k]];
             slot = hash_find(keys, cap - 1, p);
         }
+        if (A.save && slot != NONE)
+            atomicAdd(&A.save[A.pins[k]], (unsigned long long)leave_gain(A.encourage, A.wfx[h], cnt[slot]));
         bool first = slot != NONE && mn[slot] == (u32)(k - a);
         u32 bal = __ballot_sync(0xFFFFFFFFu, first);
         if (lane == 0) wsum[w] = __popc(bal);
@@ -165,6 +180,28 @@ __global__ void k_part_inbound(u32 e, const u64 *__restrict__ off, const u32 *__
         if (cdcnt[a + j] > 0) atomicAdd(&pinb[cpart[a + j]], 1ull);
 }
 
+constexpr u32 PI_SMEM_K = 8192;
+// k_part_inbound for K <= PI_SMEM_K: warps stride over the hyperedges and count into a shared
+// histogram, which the block adds to pinb once; this avoids contended global atomics on few
+// partitions.
+__global__ void k_part_inbound_smem(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ lam,
+                                    const u32 *__restrict__ cpart, const u32 *__restrict__ cdcnt, u32 K,
+                                    unsigned long long *__restrict__ pinb) {
+    extern __shared__ u32 hist[];
+    for (u32 i = threadIdx.x; i < K; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const u32 lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (u32 h = blockIdx.x * nw + (threadIdx.x >> 5); h < e; h += gridDim.x * nw) {
+        const u64 a = off[h];
+        const u32 lm = lam[h];
+        for (u32 j = lane; j < lm; j += 32)
+            if (cdcnt[a + j] > 0) atomicAdd(&hist[cpart[a + j]], 1u);
+    }
+    __syncthreads();
+    for (u32 i = threadIdx.x; i < K; i += blockDim.x)
+        if (hist[i]) atomicAdd(&pinb[i], (unsigned long long)hist[i]);
+}
+
 // ------------------------------------------------------------------ gains
 struct GainArgs {
     u32 n, omega, delta, discount, round;
@@ -179,6 +216,7 @@ struct GainArgs {
     i64 *gain;
     u32 *status;
     const u32 *dyn;  // when set: discount and round read from device memory (graph replays)
+    const i64 *save; // partition-indexed gains: each node's saving from leaving its partition
     u32 K;           // partitions: with K <= GN_DIRECT_K the tables are indexed by partition id
 };
 
@@ -204,11 +242,6 @@ __device__ __forceinline__ GainArgs gain_args_now(const GainArgs &A0) {
         A.round = A0.dyn[1];
     }
     return A;
-}
-
-__device__ __forceinline__ i64 leave_gain(int encourage, u32 w, u32 c) {
-    if (encourage) return c >= 1 ? (i64)((u64)w / ((u64)c * c)) : 0;
-    return c == 1 ? (i64)w : 0;
 }
 
 // Per-level bounds of a node's gain work: the partitions adjacent to it in any round number at
@@ -244,12 +277,25 @@ __host__ __device__ __forceinline__ u32 table_cap(u64 work, u32 cap_max) {
 // `stride` entries. A batch's hyperedge metadata loads in parallel; its census entries are then
 // flattened across the lanes (each lane finds its entry's hyperedge by a 5-step search over the
 // prefix of the batch's lambdas). saving and wtot are per-lane partial sums.
+//
+// With `trk` the block counts the distinct partitions it inserts. In a first try (limit below the
+// table size) passing the limit, or a full table, sets *ovf and the warps stop at their next batch;
+// the caller retries the node with a larger table. With trk->used the inserted slots are listed,
+// so the caller can scan and clear only those.
+struct GainTrack {
+    u32 *ndist;
+    u32 limit;
+    volatile u32 *ovf;
+    u32 *used;
+};
 __device__ __forceinline__ void gain_flat(const GainArgs &A, u32 u, u32 p, u32 *keys, unsigned long long *conn,
-                                          u32 *dconn, u32 mask, u32 first, u32 stride, i64 &saving, i64 &wtot) {
+                                          u32 *dconn, u32 mask, u32 first, u32 stride, i64 &saving, i64 &wtot,
+                                          const GainTrack *trk = nullptr) {
     const u32 lane = threadIdx.x & 31u;
     const u64 t0 = A.toff[u];
     const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
     for (u32 jb = first; jb < deg; jb += stride) {
+        if (trk && __any_sync(0xFFFFFFFFu, *trk->ovf != 0)) return;
         const u32 j = jb + lane;
         const bool has = j < deg;
         const u32 h = has ? A.touch[t0 + j] : 0;
@@ -289,6 +335,19 @@ __device__ __forceinline__ void gain_flat(const GainArgs &A, u32 u, u32 p, u32 *
             if (gain_direct(A)) {  // the slot is the partition id: no probing
                 slot = q;
                 keys[q] = q;
+            } else if (trk) {
+                bool fresh;
+                slot = hash_insert_fresh(keys, mask, q, fresh);
+                if (slot == NONE) {  // full: a first try overflows, a sized table is an error
+                    if (trk->limit <= mask) *trk->ovf = 1u;
+                    else atomicExch(A.status, DEV_HASH_FULL);
+                    continue;
+                }
+                if (fresh) {
+                    const u32 idx = atomicAdd(trk->ndist, 1u);
+                    if (trk->used) trk->used[idx] = slot;
+                    if (idx >= trk->limit) *trk->ovf = 1u;
+                }
             } else {
                 slot = hash_find_or_insert(keys, mask, q);
                 if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
@@ -336,6 +395,222 @@ constexpr u32 GN_BLOCK = 256;
 constexpr u32 GN_BLOCK_W = 4096;
 constexpr u32 GN_WARP_DEG = 256;      // incidences one warp takes; more go to a block
 constexpr u32 GN_SMALL_LEVEL = 1024;  // levels with at most this many nodes use blocks only
+constexpr u32 GM_WARP_DEG = 4096;     // incidences one warp takes in the mask gains; more go to a block
+
+// ------------------------------------------------------------------ partition-indexed gains
+// For K <= GN_DIRECT_K a hyperedge's census is also kept as two K-bit masks of MW words: the
+// partitions present, and those holding destination pins. A node's table is then MW registers
+// per lane (lane l owns partitions l, l + 32, ...), so an incidence costs O(MW) per lane whatever
+// its lambda, against lambda hash updates in the general path. The node's saving from leaving
+// its own partition comes from the census pass (Census::save); candidates, connectivity and the
+// inbound count per candidate are the same quantities the general path accumulates.
+__global__ void k_census_masks(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ lam,
+                               const u32 *__restrict__ cpart, const u32 *__restrict__ cdcnt, u32 MW,
+                               u32 *__restrict__ mask, u32 *__restrict__ dmask) {
+    const u32 h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (h >= e) return;
+    const u64 a = off[h];
+    const u32 lm = lam[h];
+    u32 mw[8], dw[8];
+#pragma unroll
+    for (u32 k = 0; k < 8; ++k) mw[k] = dw[k] = 0;
+    for (u32 j = lane; j < lm; j += 32) {
+        const u32 q = cpart[a + j], bit = 1u << (q & 31), wd = q >> 5;
+        const bool d = cdcnt[a + j] > 0;
+#pragma unroll
+        for (u32 k = 0; k < 8; ++k)
+            if (k == wd) {
+                mw[k] |= bit;
+                if (d) dw[k] |= bit;
+            }
+    }
+#pragma unroll
+    for (u32 k = 0; k < 8; ++k) {
+        if (k < MW) {
+            const u32 m = __reduce_or_sync(0xFFFFFFFFu, mw[k]), d = __reduce_or_sync(0xFFFFFFFFu, dw[k]);
+            if (lane == 0) {
+                mask[(u64)h * MW + k] = m;
+                dmask[(u64)h * MW + k] = d;
+            }
+        }
+    }
+}
+
+template <u32 MW>
+__device__ __forceinline__ void load_words(const u32 *p, u32 (&w)[MW]) {
+    if constexpr (MW == 1) {
+        w[0] = *p;
+    } else if constexpr (MW == 2) {
+        const uint2 v = *(const uint2 *)p;
+        w[0] = v.x; w[1] = v.y;
+    } else {
+#pragma unroll
+        for (u32 k = 0; k < MW; k += 4) {
+            const uint4 v = *(const uint4 *)(p + k);
+            w[k] = v.x; w[k + 1] = v.y; w[k + 2] = v.z; w[k + 3] = v.w;
+        }
+    }
+}
+template <u32 MW>
+__device__ __forceinline__ void store_words(u32 *p, const u32 (&w)[MW]) {
+    if constexpr (MW == 1) {
+        *p = w[0];
+    } else if constexpr (MW == 2) {
+        *(uint2 *)p = make_uint2(w[0], w[1]);
+    } else {
+#pragma unroll
+        for (u32 k = 0; k < MW; k += 4) *(uint4 *)(p + k) = make_uint4(w[k], w[k + 1], w[k + 2], w[k + 3]);
+    }
+}
+
+template <u32 MW>
+struct MaskAcc {
+    unsigned long long conn[MW];  // this lane's partitions: summed weights of incidences holding them
+    u32 dconn[MW];                // inbound incidences with destination pins in them
+    u32 pres[MW];                 // OR of the mask words seen (bit `lane` of word k: partition lane + 32k)
+};
+
+// Accumulate node u's incidences first, first + stride, ... in batches of 32 (one warp). Each
+// batch stages its masks in the warp's shared slots (sm, sd, sw: 32 entries), which every lane
+// then reads as broadcasts.
+template <u32 MW>
+__device__ __forceinline__ void gain_mask_acc(const GainArgs &A, const u32 *__restrict__ mask,
+                                              const u32 *__restrict__ dmask, u32 u, u32 first, u32 stride,
+                                              u32 (*sm)[MW], u32 (*sd)[MW], u32 *sw, MaskAcc<MW> &acc, i64 &wtot) {
+    const u32 lane = threadIdx.x & 31u;
+    const u64 t0 = A.toff[u];
+    const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
+    for (u32 jb = first; jb < deg; jb += stride) {
+        const u32 j = jb + lane;
+        const bool has = j < deg;
+        const u32 h = has ? A.touch[t0 + j] : 0;
+        const u32 wh = has ? A.wfx[h] : 0;
+        wtot += wh;
+        u32 mw[MW], dw[MW];
+#pragma unroll
+        for (u32 k = 0; k < MW; ++k) mw[k] = dw[k] = 0;
+        if (has) load_words<MW>(mask + (u64)h * MW, mw);
+        if (has && j < nin_u) load_words<MW>(dmask + (u64)h * MW, dw);
+        store_words<MW>(sm[lane], mw);
+        store_words<MW>(sd[lane], dw);
+        sw[lane] = wh;
+        __syncwarp();
+        const u32 chunk = (deg - jb) < 32 ? (deg - jb) : 32;
+        for (u32 t = 0; t < chunk; ++t) {
+            const u32 wt = sw[t];
+            u32 mk[MW], dk[MW];
+            load_words<MW>(sm[t], mk);
+            load_words<MW>(sd[t], dk);
+#pragma unroll
+            for (u32 k = 0; k < MW; ++k) {
+                if ((mk[k] >> lane) & 1u) acc.conn[k] += wt;
+                acc.dconn[k] += (dk[k] >> lane) & 1u;
+                acc.pres[k] |= mk[k];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <u32 MW>
+__device__ __forceinline__ Cand mask_best(const GainArgs &A, u32 u, u32 p, const MaskAcc<MW> &acc, i64 saving,
+                                          i64 wtot) {
+    const u32 lane = threadIdx.x & 31u;
+    Cand best{INT64_MIN, 0};
+#pragma unroll
+    for (u32 k = 0; k < MW; ++k) {
+        const u32 q = lane + 32 * k;
+        if (q < A.K && q != p && ((acc.pres[k] >> lane) & 1u)) {
+            const Cand c = gain_candidate(A, u, q, acc.conn[k], acc.dconn[k], saving, wtot);
+            if (cand_better(c, best)) best = c;
+        }
+    }
+    return warp_best(best);
+}
+
+__device__ __forceinline__ void write_move(const GainArgs &A, u32 u, const Cand &b) {
+    if (b.g != INT64_MIN && b.g > 0) {
+        A.target[u] = ~(u32)b.tie;
+        A.gain[u] = b.g;
+    } else {
+        A.target[u] = NONE;
+        A.gain[u] = 0;
+    }
+}
+
+// One warp per node.
+template <u32 MW>
+__global__ void __launch_bounds__(GN_WARPS * 32) k_gain_mask_warp(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                                 const u32 *__restrict__ mask,
+                                                                 const u32 *__restrict__ dmask) {
+    const GainArgs A = gain_args_now(A0);
+    __shared__ __align__(16) u32 sm[GN_WARPS][32][MW], sd[GN_WARPS][32][MW];
+    __shared__ u32 sw[GN_WARPS][32];
+    const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 idx = blockIdx.x * GN_WARPS + w;
+    if (idx >= nl) return;
+    const u32 u = list[idx], p = A.part[u];
+    MaskAcc<MW> acc;
+#pragma unroll
+    for (u32 k = 0; k < MW; ++k) { acc.conn[k] = 0; acc.dconn[k] = 0; acc.pres[k] = 0; }
+    i64 wtot = 0;
+    gain_mask_acc<MW>(A, mask, dmask, u, 0, 32, sm[w], sd[w], sw[w], acc, wtot);
+    wtot = warp_sum(wtot);
+    const Cand best = mask_best<MW>(A, u, p, acc, A.save[u], wtot);
+    if (lane == 0) write_move(A, u, best);
+}
+
+// One block per node (its warps split the incidences), for heavy nodes and small levels; the
+// warps' tables are summed in shared memory.
+template <u32 MW>
+__global__ void __launch_bounds__(GN_BLOCK) k_gain_mask_block(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                             const u32 *__restrict__ mask,
+                                                             const u32 *__restrict__ dmask) {
+    constexpr u32 NW = GN_BLOCK / 32;
+    const GainArgs A = gain_args_now(A0);
+    __shared__ __align__(16) u32 sm[NW][32][MW], sd[NW][32][MW];
+    __shared__ u32 sw[NW][32];
+    __shared__ unsigned long long rc[MW][32];
+    __shared__ u32 rd[MW][32], rp[MW];
+    __shared__ i64 rw[NW];
+    const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (u32 i = threadIdx.x; i < MW * 32; i += blockDim.x) { rc[i / 32][i % 32] = 0; rd[i / 32][i % 32] = 0; }
+    if (threadIdx.x < MW) rp[threadIdx.x] = 0;
+    __syncthreads();
+    for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
+        const u32 u = list[idx], p = A.part[u];
+        MaskAcc<MW> acc;
+#pragma unroll
+        for (u32 k = 0; k < MW; ++k) { acc.conn[k] = 0; acc.dconn[k] = 0; acc.pres[k] = 0; }
+        i64 wtot = 0;
+        gain_mask_acc<MW>(A, mask, dmask, u, 32 * w, GN_BLOCK, sm[w], sd[w], sw[w], acc, wtot);
+        wtot = warp_sum(wtot);
+#pragma unroll
+        for (u32 k = 0; k < MW; ++k) {
+            if (acc.conn[k]) atomicAdd(&rc[k][lane], acc.conn[k]);
+            if (acc.dconn[k]) atomicAdd(&rd[k][lane], acc.dconn[k]);
+            if (lane == 0 && acc.pres[k]) atomicOr(&rp[k], acc.pres[k]);
+        }
+        if (lane == 0) rw[w] = wtot;
+        __syncthreads();
+        if (w == 0) {
+#pragma unroll
+            for (u32 k = 0; k < MW; ++k) {
+                acc.conn[k] = rc[k][lane];
+                acc.dconn[k] = rd[k][lane];
+                acc.pres[k] = rp[k];
+            }
+            wtot = 0;
+            for (u32 i = 0; i < NW; ++i) wtot += rw[i];
+            const Cand best = mask_best<MW>(A, u, p, acc, A.save[u], wtot);
+            if (lane == 0) write_move(A, u, best);
+        }
+        __syncthreads();  // warp 0 has read the sums: clear them for the next node
+        for (u32 i = threadIdx.x; i < MW * 32; i += blockDim.x) { rc[i / 32][i % 32] = 0; rd[i / 32][i % 32] = 0; }
+        if (threadIdx.x < MW) rp[threadIdx.x] = 0;
+        __syncthreads();
+    }
+}
 
 __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const u32 *__restrict__ list, u32 nl,
                                                              const u64 *__restrict__ work) {
@@ -374,43 +649,83 @@ __global__ void __launch_bounds__(GN_WARPS * 32) k_gain_warp(GainArgs A0, const 
     }
 }
 
-__global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 *__restrict__ list, u32 nl, u32 cap_max,
-                                                        u32 *gtab, const u64 *__restrict__ work) {
+// One block per node. Three table modes:
+// - shared, sized (gtab null, try_limit 0): the node's table bound fits in shared memory;
+// - shared, first try (try_limit > 0): a cap_max-slot shared table for nodes whose bound does not
+//   fit; a node with more than try_limit distinct partitions is appended to retry / *nretry;
+// - global (gtab set): this block's slice of gtab, sized by the bound. Inserted slots are listed
+//   in this block's slice of gused, so candidates are read from and cleared in those slots only;
+//   the slice is cleared once at the start.
+// With dnl set, the node count is read from device memory.
+__global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                        const u32 *__restrict__ dnl, u32 cap_max, u32 *gtab,
+                                                        u32 *gused, const u64 *__restrict__ work, u32 try_limit,
+                                                        u32 *__restrict__ retry, u32 *__restrict__ nretry) {
     const GainArgs A = gain_args_now(A0);
     extern __shared__ unsigned long long dyn64[];
     __shared__ i64 red[2][32];
     __shared__ Cand cred[32];
+    __shared__ u32 ndist, ovf;
+    if (dnl) nl = *dnl;
+    // this block's global slice: conn u64 [cap_max], keys and dconn u32 [cap_max]; a node uses
+    // the first `cap` slots of each, and leaves every slot empty again when it is done
+    u32 *gbase = gtab ? gtab + (u64)blockIdx.x * 4 * cap_max : nullptr;
+    u32 *used = gtab ? gused + (u64)blockIdx.x * cap_max : nullptr;
+    if (gtab && blockIdx.x < nl) {
+        for (u32 i = threadIdx.x; i < 2 * cap_max; i += blockDim.x) gbase[i] = 0;
+        for (u32 i = threadIdx.x; i < cap_max; i += blockDim.x) { gbase[2 * cap_max + i] = NONE; gbase[3 * cap_max + i] = 0; }
+    }
     for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
         const u32 u = list[idx], p = A.part[u];
         unsigned long long *conn;
         u32 *keys, *dconn;
-        const u32 cap = gain_cap(A, work[u], cap_max);
+        const u32 cap = try_limit ? cap_max : gain_cap(A, work[u], cap_max);
         if (gtab) {
-            u32 *base = gtab + (u64)blockIdx.x * 4 * cap_max;  // this block's slice
-            conn = (unsigned long long *)base;
-            keys = base + 2 * cap;
-            dconn = keys + cap;
+            conn = (unsigned long long *)gbase;
+            keys = gbase + 2 * cap_max;
+            dconn = keys + cap_max;
         } else {
             conn = dyn64;
             keys = (u32 *)(dyn64 + cap);
             dconn = keys + cap;
+            for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
         }
-        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; dconn[i] = 0; conn[i] = 0; }
+        if (threadIdx.x == 0) { ndist = 0; ovf = 0; }
         __syncthreads();
+        const bool track = (try_limit || gtab) && !gain_direct(A);
+        const GainTrack trk{&ndist, try_limit ? try_limit : cap, &ovf, used};
         i64 saving = 0, wtot = 0;
-        gain_flat(A, u, p, keys, conn, dconn, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x, saving, wtot);
+        gain_flat(A, u, p, keys, conn, dconn, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x, saving, wtot,
+                  track ? &trk : nullptr);
         saving = warp_sum(saving);
         wtot = warp_sum(wtot);
         if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = saving; red[1][threadIdx.x >> 5] = wtot; }
         __syncthreads();
+        if (ovf) {  // first try overflowed: the global tier takes the node
+            if (threadIdx.x == 0) retry[atomicAdd(nretry, 1u)] = u;
+            __syncthreads();
+            continue;
+        }
         saving = 0;
         wtot = 0;
         for (u32 i = 0; i < blockDim.x / 32; ++i) { saving += red[0][i]; wtot += red[1][i]; }
         Cand best{INT64_MIN, 0};
-        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) {
+        const bool listed = track && used;
+        const u32 nscan = listed ? ndist : cap;
+        for (u32 t = threadIdx.x; t < nscan; t += blockDim.x) {
+            const u32 i = listed ? used[t] : t;
             if (keys[i] == NONE) continue;
             Cand c = gain_candidate(A, u, keys[i], conn[i], dconn[i], saving, wtot);
             if (cand_better(c, best)) best = c;
+        }
+        if (gtab) {
+            __syncthreads();  // every candidate is read before the slots are emptied
+            for (u32 t = threadIdx.x; t < nscan; t += blockDim.x) {
+                const u32 i = listed ? used[t] : t;
+                keys[i] = NONE;
+                conn[i] = 0;
+                dconn[i] = 0;
+            }
         }
         best = warp_best(best);
         if ((threadIdx.x & 31) == 0) cred[threadIdx.x >> 5] = best;
@@ -449,15 +764,17 @@ __global__ void k_list_max(const u32 *__restrict__ list, u32 nl, const u64 *__re
 // table in shared memory, 2 = one block with the table in global scratch. Levels of at most
 // GN_SMALL_LEVEL nodes use no warp tier: their few nodes carry long census chains, which a block
 // splits over its warps while the rest of the GPU would idle anyway.
-__device__ __forceinline__ u32 gain_tier(u32 n, u64 wk, u64 deg) {
+__device__ __forceinline__ u32 gain_tier(u32 n, u32 K, u64 wk, u64 deg) {
+    if (K <= GN_DIRECT_K)  // partition-indexed gains: a warp or a block, by incidences
+        return (n > GN_SMALL_LEVEL && deg <= GM_WARP_DEG) ? 0u : 1u;
     if (wk > GN_BLOCK_W) return 2u;
     return (n > GN_SMALL_LEVEL && wk <= GN_WARP_W && deg <= GN_WARP_DEG) ? 0u : 1u;
 }
-__global__ void k_tier(u32 n, const u64 *__restrict__ work, const u64 *__restrict__ toff, u32 tier,
+__global__ void k_tier(u32 n, u32 K, const u64 *__restrict__ work, const u64 *__restrict__ toff, u32 tier,
                        u32 *__restrict__ flag) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
-    flag[u] = gain_tier(n, work[u], toff[u + 1] - toff[u]) == tier ? 1u : 0u;
+    flag[u] = gain_tier(n, K, work[u], toff[u + 1] - toff[u]) == tier ? 1u : 0u;
 }
 
 // ------------------------------------------------------------------ ranking
@@ -519,12 +836,14 @@ __device__ __forceinline__ void cascade_fill(const CascadeArgs &A, u64 a, u32 lm
     }
 }
 
-__device__ __forceinline__ void emit_transition(const CascadeArgs &A, u32 p, u32 r, int32_t d) {
-    const u32 s = atomicAdd(A.dT, 1u);
+__device__ __forceinline__ void emit_at(const CascadeArgs &A, u32 s, u32 p, u32 r, int32_t d) {
     if (s >= A.tcap) { atomicExch(A.status, DEV_BAD_INDEX); return; }
     A.tp[s] = p;
     A.tr[s] = r;
     A.tdv[s] = d;
+}
+__device__ __forceinline__ void emit_transition(const CascadeArgs &A, u32 p, u32 r, int32_t d) {
+    emit_at(A, atomicAdd(A.dT, 1u), p, r, d);
 }
 
 // Table slots of every mover's source and target partition, sl[i] = slot(p) | slot(q) << 16,
@@ -550,6 +869,7 @@ __device__ __forceinline__ void cascade_slots(const CascadeArgs &A, const u64 *m
 // node; tc / td hold the hyperedge's pins / destination pins per partition (hash slots in tk,
 // or the partition id itself for direct tables). With sl the slots come precomputed from
 // cascade_slots; without it (hashed tables too large for 16-bit slots) they are looked up here.
+// One thread; cascade_sweep_warp is the warp-wide form used wherever the slots fit 16 bits.
 __device__ void cascade_sweep(const CascadeArgs &A, u32 h, const u64 *mv, const u32 *sl, u32 m, u32 *tk, u32 *tc,
                               u32 *td, u32 mask) {
     const u32 w = A.wfx[h];
@@ -598,6 +918,71 @@ __device__ __forceinline__ u32 cascade_cap32(u32 lm, u32 m) {
 
 // Hyperedges with at most CC_MOV movers, one warp each (hashed tables also need at most CC_TAB
 // slots); the others are appended to `big` for the block kernel.
+// The same sweep with a whole warp, 32 movers at a time (slots from cascade_slots required). The
+// counts a mover sees are the table's counts before its chunk plus what the chunk's earlier lanes
+// did to its two partitions: leaves of the same source (match_any), joins of the same target
+// (match_any), and the cross terms, lanes whose target is its source or whose source is its
+// target (one shuffle pass over the chunk). The tables are then updated by the whole chunk at once.
+// Equal to the sequential sweep: the counts are exact prefix sums, and transitions are a set.
+__device__ void cascade_sweep_warp(const CascadeArgs &A, u32 h, const u64 *mv, const u32 *sl, u32 m, const u32 *tk,
+                                   u32 *tc, u32 *td) {
+    const u32 lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    const u32 w = A.wfx[h];
+    const bool direct = cascade_direct(A);
+    for (u32 base = 0; base < m; base += 32) {
+        const u32 i = base + lane;
+        const bool act = i < m;
+        const u64 e = act ? mv[i] : 0;
+        // inactive lanes get slots no table has (slots are below 65536), distinct per lane
+        const u32 sp = act ? (sl[i] & 0xFFFFu) : 0x10000u + lane, sq = act ? (sl[i] >> 16) : 0x20000u + lane;
+        const bool dst = act && ((u32)e & MV_DST);
+        const u32 dmask = __ballot_sync(0xFFFFFFFFu, dst);
+        const u32 m_pp = __match_any_sync(0xFFFFFFFFu, sp), m_qq = __match_any_sync(0xFFFFFFFFu, sq);
+        u32 m_qp = 0, m_pq = 0;  // lanes whose target is my source / whose source is my target
+#pragma unroll 8
+        for (u32 j = 0; j < 32; ++j) {
+            const u32 spj = __shfl_sync(0xFFFFFFFFu, sp, j), sqj = __shfl_sync(0xFFFFFFFFu, sq, j);
+            m_qp |= (u32)(sqj == sp) << j;
+            m_pq |= (u32)(spj == sq) << j;
+        }
+        const int before_p = __popc(m_qp & lt) - __popc(m_pp & lt);
+        const int before_q = __popc(m_qq & lt) - __popc(m_pq & lt);
+        if (act) {
+            const u32 cp = (u32)((int)tc[sp] + before_p), cq = (u32)((int)tc[sq] + before_q);
+            const i64 d = leave_gain(A.encourage, w, cp) - (cq == 0 ? (i64)w : 0);
+            atomicAdd(&A.g2[(u32)e & ~MV_DST], (unsigned long long)d);
+        }
+        if (A.track) {  // warp-uniform
+            bool ep = false, eq = false;
+            if (dst) {
+                const int dp = __popc(m_qp & lt & dmask) - __popc(m_pp & lt & dmask);
+                const int dq = __popc(m_qq & lt & dmask) - __popc(m_pq & lt & dmask);
+                ep = (int)td[sp] + dp == 1;
+                eq = (int)td[sq] + dq == 0;
+            }
+            // one reservation per chunk: p-transitions first, then q-transitions
+            const u32 bp = __ballot_sync(0xFFFFFFFFu, ep), bq = __ballot_sync(0xFFFFFFFFu, eq);
+            const u32 tot = __popc(bp) + __popc(bq);
+            u32 s0 = 0;
+            if (lane == 0 && tot) s0 = atomicAdd(A.dT, tot);
+            s0 = __shfl_sync(0xFFFFFFFFu, s0, 0);
+            const u32 r = (u32)(e >> 32);
+            if (ep) emit_at(A, s0 + __popc(bp & lt), direct ? sp : tk[sp], r, -1);
+            if (eq) emit_at(A, s0 + __popc(bp) + __popc(bq & lt), direct ? sq : tk[sq], r, +1);
+        }
+        __syncwarp();
+        if (act) {
+            atomicSub(&tc[sp], 1u);
+            atomicAdd(&tc[sq], 1u);
+            if (dst) {
+                atomicSub(&td[sp], 1u);
+                atomicAdd(&td[sq], 1u);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__restrict__ nbig) {
     __shared__ u64 mvs[CC_WARPS][CC_MOV];
     __shared__ u32 sl[CC_WARPS][CC_MOV];
@@ -647,7 +1032,7 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__rest
     __syncwarp();
     cascade_slots(A, mvs[w], sl[w], m, tk[w], cap, lane, 32);
     __syncwarp();
-    if (lane == 0) cascade_sweep(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], cap - 1);
+    cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w]);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -671,7 +1056,8 @@ __device__ void block_bitonic_u64(u64 *buf, u32 P) {
 
 constexpr u32 CB_THREADS = 128;
 constexpr u32 CB_MOV_MAX = 2048;  // movers of the block kernel, in shared memory
-constexpr u32 CB_TAB_HASH = 1024; // hashed table slots of the block kernel
+constexpr u32 CB_TAB_HASH = 8192; // hashed table slots of the block kernel, at most
+constexpr size_t CB_DYN_MAX = (size_t)CB_MOV_MAX * 12 + (size_t)CB_TAB_HASH * 12;
 
 // Gather the movers of hyperedge h (rank << 32 | dst flag | node) into mvs[0, min(m, lim)) with
 // the whole block; returns m (all of them, counted past lim). Ends with the block synchronised.
@@ -707,7 +1093,11 @@ __device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u
         cascade_slots(A, mvs, sl, m, tk, cap, threadIdx.x, blockDim.x);
         __syncthreads();
     }
-    if (threadIdx.x == 0) cascade_sweep(A, h, mvs, sl, m, tk, tc, td, cap - 1);
+    if (sl) {
+        if (threadIdx.x < 32) cascade_sweep_warp(A, h, mvs, sl, m, tk, tc, td);
+    } else if (threadIdx.x == 0) {
+        cascade_sweep(A, h, mvs, sl, m, tk, tc, td, cap - 1);
+    }
     __syncthreads();
 }
 
@@ -936,6 +1326,7 @@ GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp,
     A.toff = L.toff; A.touch = L.touch; A.nin = L.nin; A.nsize = L.nsize; A.part = part;
     A.psize = psize; A.pinb = pinb; A.target = target; A.gain = gain; A.status = status;
     A.dyn = nullptr;
+    A.save = cs.save;
     return A;
 }
 
@@ -974,20 +1365,21 @@ static u32 cascade_block_movers() {
 void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_census_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 2 * CS_BLOCK_CAP * 4));
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
+    AXC_CUDA(cudaFuncSetAttribute(k_cascade_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_DYN_MAX));
 }
 
 __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
                                unsigned long long *__restrict__ out);
 
 // Largest gain-work bound over all nodes (out[0]) and over the block tier (out[1]).
-__global__ void k_tier_max(u32 n, const u64 *__restrict__ work, const u64 *__restrict__ toff,
+__global__ void k_tier_max(u32 n, u32 K, const u64 *__restrict__ work, const u64 *__restrict__ toff,
                            unsigned long long *__restrict__ out) {
     u32 u = blockIdx.x * blockDim.x + threadIdx.x;
     u64 all = 0, blk = 0;
     if (u < n) {
         const u64 wk = work[u], deg = toff[u + 1] - toff[u];
         all = wk;
-        if (gain_tier(n, wk, deg) == 1u) blk = wk;
+        if (gain_tier(n, K, wk, deg) == 1u) blk = wk;
     }
     all = warp_max_u64(all);
     blk = warp_max_u64(blk);
@@ -1024,10 +1416,10 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
         u32 *flag = c.arena.alloc<u32>(n);
         for (u32 t = 0; t < 3; ++t) {
             lp.ntier[t] = c.arena.alloc<u32>(n);
-            LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, work, L.toff, t, flag);
+            LAUNCH(c, k_tier, cdiv(n, 256), 256, 0, n, K, work, L.toff, t, flag);
             compact_indices_dn(c, flag, lp.ntier[t], n, (u32 *)(dc + 2 + t));
         }
-        LAUNCH(c, k_tier_max, cdiv(n, 256), 256, 0, n, work, L.toff, (unsigned long long *)(dc + 6));
+        LAUNCH(c, k_tier_max, cdiv(n, 256), 256, 0, n, K, work, L.toff, (unsigned long long *)(dc + 6));
     }
     u64 h[10];
     fetch(c, h, dc, 80);
@@ -1060,7 +1452,8 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
 static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *part, Census &cs) {
     cs.beg = L.off;
     if (L.e == 0) return;
-    CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status};
+    CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status,
+                 (unsigned long long *)cs.save, cs.wfx, cs.encourage};
     LAUNCH(c, k_census_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A);
     if (lp.n_hblock)
         LAUNCH(c, k_census_block, lp.n_hblock, 256, 4 * 2 * CS_BLOCK_CAP * 4, lp.hblock, lp.n_hblock, A,
@@ -1088,8 +1481,39 @@ static Census alloc_census(Ctx &c, const DLevel &L) {
 // move, gain and rank).
 static u64 gain_bytes(const LevelPrep &lp, int t) { return 8 * lp.tier_deg[t] + 16 * (u64)lp.ncount[t]; }
 
-static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainArgs &A) {
+// Distinct partitions a node may reach in the first try of the heavy gain tier: 3/4 of the
+// table, or fewer when the environment variable AXC_GAIN_TRY_LIMIT asks for it (at least 1),
+// which sends more nodes to the global retry; the tests use it to reach that path on small inputs.
+static u32 gain_try_limit(u32 cap) {
+    const u32 lim = cap / 4 * 3;
+    const char *s = std::getenv("AXC_GAIN_TRY_LIMIT");
+    if (!s || !*s) return lim;
+    const unsigned long v = std::strtoul(s, nullptr, 10);
+    return v < 1 ? 1u : (v < lim ? (u32)v : lim);
+}
+
+template <u32 MW>
+static void run_gains_masked(Ctx &c, const LevelPrep &lp, const GainArgs &A, const Census &cs) {
+    if (lp.ncount[0])
+        LAUNCH(c, k_gain_mask_warp<MW>, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0],
+               cs.mask, cs.dmask);
+    if (lp.ncount[1])
+        LAUNCH(c, k_gain_mask_block<MW>, lp.ncount[1], GN_BLOCK, 0, A, lp.ntier[1], lp.ncount[1], cs.mask, cs.dmask);
+}
+
+static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainArgs &A, const Census &cs) {
     fill_u32(c, A.target, NONE, L.n);
+    if (cs.mask) {  // partition-indexed gains (K <= GN_DIRECT_K)
+        if (c.profiling("k_gain_mask_warp")) c.prof_bytes += gain_bytes(lp, 0);
+        if (c.profiling("k_gain_mask_block")) c.prof_bytes += gain_bytes(lp, 1);
+        switch (cs.mw) {
+            case 1: run_gains_masked<1>(c, lp, A, cs); break;
+            case 2: run_gains_masked<2>(c, lp, A, cs); break;
+            case 4: run_gains_masked<4>(c, lp, A, cs); break;
+            default: run_gains_masked<8>(c, lp, A, cs); break;
+        }
+        return;
+    }
     if (c.profiling("k_gain_warp") && lp.ncount[0]) c.prof_bytes += gain_bytes(lp, 0);
     if (c.profiling("k_gain_block")) c.prof_bytes += gain_bytes(lp, 1) + gain_bytes(lp, 2);
     LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
@@ -1098,16 +1522,31 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
         u32 cap1 = table_cap(lp.block_work_max, 2 * GN_BLOCK_W);
         if (A.K <= GN_DIRECT_K)  // indexed by partition id: K slots (rounded up) per node
             while (cap1 < A.K) cap1 <<= 1;
-        LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, cap1 * 16, A, lp.ntier[1], lp.ncount[1], cap1, (u32 *)nullptr,
-               lp.work);
+        LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, cap1 * 16, A, lp.ntier[1], lp.ncount[1], (const u32 *)nullptr,
+               cap1, (u32 *)nullptr, (u32 *)nullptr, lp.work, 0u, (u32 *)nullptr, (u32 *)nullptr);
     }
     if (lp.ncount[2]) {
         size_t m = c.arena.mark();
+        const u32 *heavy = lp.ntier[2];
+        const u32 *dn = nullptr;
+        if (A.K > GN_DIRECT_K) {
+            // Bounds overestimate: partitions recur across a node's hyperedges. First try with the
+            // largest shared table; a node with more than 3/4 of its slots distinct is retried.
+            const u32 cap_try = 2 * GN_BLOCK_W;
+            u32 *retry = c.arena.alloc<u32>(lp.ncount[2]), *nretry = c.arena.alloc<u32>(1);
+            AXC_CUDA(cudaMemsetAsync(nretry, 0, 4, c.stream));
+            LAUNCH(c, k_gain_block, lp.ncount[2], GN_BLOCK, cap_try * 16, A, lp.ntier[2], lp.ncount[2],
+                   (const u32 *)nullptr, cap_try, (u32 *)nullptr, (u32 *)nullptr, lp.work, gain_try_limit(cap_try), retry,
+                   nretry);
+            heavy = retry;
+            dn = nretry;
+        }
         u32 cap = 64;
         while (cap < 2 * lp.heavy_work_max && cap < (1u << 28)) cap <<= 1;
         u32 grid = lp.ncount[2] < (u32)c.sms * 2 ? lp.ncount[2] : (u32)c.sms * 2;
-        u32 *gtab = c.arena.alloc<u32>((u64)grid * 4 * cap);
-        LAUNCH(c, k_gain_block, grid, GN_BLOCK, 0, A, lp.ntier[2], lp.ncount[2], cap, gtab, lp.work);
+        u32 *gtab = c.arena.alloc<u32>((u64)grid * 4 * cap), *gused = c.arena.alloc<u32>((u64)grid * cap);
+        LAUNCH(c, k_gain_block, grid, GN_BLOCK, 0, A, heavy, lp.ncount[2], dn, cap, gtab, gused, lp.work, 0u,
+               (u32 *)nullptr, (u32 *)nullptr);
         c.arena.release(m);
     }
 }
@@ -1142,22 +1581,63 @@ void part_sizes(Ctx &c, u32 n, const u32 *part, const u32 *nsize, u64 *psize, u3
 }
 void part_inbound(Ctx &c, const DLevel &L, const Census &cs, u64 *pinb, u32 K) {
     AXC_CUDA(cudaMemsetAsync(pinb, 0, (size_t)K * 8, c.stream));
-    if (L.e)
+    if (L.e && K <= PI_SMEM_K) {  // per-block counts in shared memory, one global add per partition
+        const u32 grid = std::min<u32>(cdiv(L.e, 256 / 32), 2 * (u32)c.sms);
+        LAUNCH(c, k_part_inbound_smem, grid, 256, (size_t)K * 4, L.e, L.off, cs.lam, cs.part, cs.dcnt, K,
+               (unsigned long long *)pinb);
+    } else if (L.e)
         LAUNCH(c, k_part_inbound, cdiv((u64)L.e * 32, 256), 256, 0, L.e, L.off, cs.lam, cs.part, cs.dcnt,
                (unsigned long long *)pinb);
+}
+
+// Whether a round needs the partitions' inbound counts. With no inbound limit (delta 2^31 - 1,
+// k-way) the inbound check pinb[q] + nin[u] - dc > delta never holds while the level has fewer
+// than 2^30 hyperedges (both terms are at most e), so zero counts decide it the same way.
+static bool inbound_binds(const DLevel &L, const RefineParams &rp) {
+    return rp.delta < 0x7FFFFFFFu || (u64)L.e >= (1ull << 30);
+}
+
+// Mask words per hyperedge for K partitions: 1, 2, 4 or 8.
+static u32 mask_words(u32 K) {
+    u32 mw = 1;
+    while (32 * mw < K) mw <<= 1;
+    return mw;
+}
+
+// The round's census, with the extras of the partition-indexed gains when K <= GN_DIRECT_K:
+// each node's saving (pushed by the census pass) and the per-hyperedge masks.
+static Census census_for_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
+                               const u32 *part) {
+    Census cs = alloc_census(c, L);
+    const bool direct = rp.K <= GN_DIRECT_K;
+    if (direct) {
+        cs.save = c.arena.alloc<i64>(L.n ? L.n : 1);
+        AXC_CUDA(cudaMemsetAsync(cs.save, 0, (size_t)L.n * 8, c.stream));
+        cs.wfx = wfx;
+        cs.encourage = rp.encourage ? 1 : 0;
+    }
+    run_census(c, L, lp, part, cs);
+    if (direct) {
+        cs.mw = mask_words(rp.K);
+        cs.mask = c.arena.alloc<u32>((u64)(L.e ? L.e : 1) * cs.mw);
+        cs.dmask = c.arena.alloc<u32>((u64)(L.e ? L.e : 1) * cs.mw);
+        if (L.e)
+            LAUNCH(c, k_census_masks, cdiv((u64)L.e * 32, 256), 256, 0, L.e, L.off, cs.lam, cs.part, cs.dcnt, cs.mw,
+                   cs.mask, cs.dmask);
+    }
+    return cs;
 }
 
 void refine_gains_only(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, const u32 *part,
                        u32 discount, u32 round, u32 *target, i64 *gain) {
     size_t m = c.arena.mark();
     LevelPrep lp = prepare_level(c, L, wfx, rp.K);
-    Census cs = alloc_census(c, L);
-    run_census(c, L, lp, part, cs);
+    Census cs = census_for_gains(c, L, lp, wfx, rp, part);
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
     part_sizes(c, L.n, part, L.nsize, psize, rp.K);
     part_inbound(c, L, cs, pinb, rp.K);
     GainArgs A = make_gain_args(L, wfx, rp, cs, part, psize, pinb, discount, round, target, gain, c.d_status);
-    run_gains(c, L, lp, A);
+    run_gains(c, L, lp, A, cs);
     check_status(c);
     c.arena.release(m);
 }
@@ -1171,16 +1651,19 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     const u32 n = L.n;
     u32 *apply = c.arena.alloc<u32>(1);
     keep = c.arena.mark();
-    Census cs = alloc_census(c, L);
-    run_census(c, L, lp, part, cs);
+    Census cs = census_for_gains(c, L, lp, wfx, rp, part);
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
     part_sizes(c, n, part, L.nsize, psize, rp.K);
-    part_inbound(c, L, cs, pinb, rp.K);
+    if (inbound_binds(L, rp)) {
+        part_inbound(c, L, cs, pinb, rp.K);
+    } else {
+        AXC_CUDA(cudaMemsetAsync(pinb, 0, (size_t)rp.K * 8, c.stream));
+    }
     u32 *target = c.arena.alloc<u32>(n);
     i64 *gain = c.arena.alloc<i64>(n);
     GainArgs A = make_gain_args(L, wfx, rp, cs, part, psize, pinb, discount, round, target, gain, c.d_status);
     A.dyn = dyn;
-    run_gains(c, L, lp, A);
+    run_gains(c, L, lp, A, cs);
     // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
     // [3] cascade hyperedges for the block kernel, [4] for the scratch kernel
     u32 *cnt = c.arena.alloc<u32>(8);
@@ -1235,7 +1718,11 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
             // block kernel: shared memory sized by the level's largest hyperedge, all resident blocks
             u32 smov = 128;
             while (smov < lp.max_len && smov < cascade_block_movers()) smov <<= 1;
-            const u32 stab = direct ? std::max(rp.K, 32u) : CB_TAB_HASH;
+            // hashed tables: sized for the level's largest hyperedge within the block's limit
+            const u32 stab = direct ? std::max(rp.K, 32u)
+                                    : (u32)std::min<u64>(cascade_cap(std::min<u64>(lp.max_len, rp.K),
+                                                                     std::min<u64>(lp.max_len, smov)),
+                                                         CB_TAB_HASH);
             const size_t dyn = (size_t)smov * 12 + (size_t)stab * 12;
             int per_sm = 1;
             AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade_block, CB_THREADS, dyn));
@@ -1245,7 +1732,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
             // movers, slots and tables per block, at most 1 GiB in all
             u64 mv_cap = 1;
             while (mv_cap < lp.max_len) mv_cap <<= 1;
-            const u64 tab_cap = direct ? stab : cascade_cap(lp.max_len, lp.max_len);
+            const u64 tab_cap = direct ? stab : cascade_cap(std::min<u64>(lp.max_len, rp.K), lp.max_len);
             if (mv_cap > smov || tab_cap > stab) {
                 const u64 per_block = mv_cap * 12 + tab_cap * 12;
                 const u32 gh = (u32)std::max<u64>(1, std::min<u64>((u64)c.sms, (1ull << 30) / per_block));

@@ -148,6 +148,24 @@ def test_cascade_kernels_match_oracle(ctx, monkeypatch, i, block_movers):
         assert st.num_parts > 256
 
 
+# Nodes whose gain-table bound passes 4096 slots (here K = 5000 partitions of two neurons and about
+# 80 inbound hyperedges of about 80 pins) first try a shared-memory table and fall back to a
+# global one when they reach too many distinct partitions. AXC_GAIN_TRY_LIMIT=16 makes nearly
+# every such node fall back.
+@pytest.mark.parametrize("try_limit", [None, "16"])
+def test_heavy_gain_tier_matches_oracle(ctx, monkeypatch, try_limit):
+    g = ax.gen_snn(4, 2500, 80, 0.7, 300, 0.7, 31)
+    p = ax.params_incc(2, 4096, 1048576, cnc=4, rfr=4)
+    if try_limit is None:
+        monkeypatch.delenv("AXC_GAIN_TRY_LIMIT", raising=False)
+    else:
+        monkeypatch.setenv("AXC_GAIN_TRY_LIMIT", try_limit)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1 and st.num_parts > 4096
+
+
 @pytest.mark.parametrize("name,cnc", [("snn_4x64.snn", 4), ("circ_2k.hgr", 8), ("snn_5x40_ln.snn", 2)])
 def test_matching_matches_oracle(ctx, name, cnc):
     g = dedup(golden(name))

@@ -53,6 +53,48 @@ def test_writer_roundtrip(tmp_path, ext):
         np.testing.assert_array_equal(h.nsrc, g.nsrc)
 
 
+@pytest.mark.parametrize("fmt", [0, 1, 11])
+def test_parallel_hgr_parse_matches_line_reader(tmp_path, fmt):
+    """The .hgr reader splits the text over threads; a large file with comments, blank and
+    CRLF lines, tabs, singleton nets, weights and trailing lines must read exactly as the
+    oracle's line-by-line restatement of the reference reader reads it."""
+    rng = np.random.default_rng(fmt)
+    g = ax.gen_circuit(40000, 44000, 2, 64, 2.5, 0.9, 0.02, 9)
+    lines = [f"% generated\n", f"{g.e + 50} {g.n} {fmt}\n" if fmt else f"{g.e + 50} {g.n}\n"]
+    nets = [g.pins[g.off[i]:g.off[i + 1]] + 1 for i in range(g.e)]
+    nets += [np.array([rng.integers(1, g.n + 1)]) for _ in range(50)]  # singletons: skipped
+    order = rng.permutation(len(nets))
+    for i in order:
+        toks = " ".join(map(str, nets[i].tolist()))
+        if fmt in (1, 11):
+            toks = f"{rng.integers(1, 9) * 0.5} " + toks
+        r = rng.random()
+        if r < 0.05:
+            lines.append("\n")
+        elif r < 0.08:
+            lines.append("  % a comment line\n")
+        if r < 0.3:
+            toks = "\t " + toks.replace(" ", "\t", 3)
+        lines.append(toks + ("\r\n" if r > 0.9 else "\n"))
+    lines += [f"{i + 1}\n" for i in range(5)]  # vertex weights (fmt 10/11) or junk: ignored
+    p = tmp_path / "big.hgr"
+    p.write_text("".join(lines))
+    h = ax.read(str(p))
+    n, off, pins, ns, w = O.read(str(p))
+    assert h.n == n and h.e == len(off) - 1
+    np.testing.assert_array_equal(h.off, off)
+    np.testing.assert_array_equal(h.pins, pins)
+    np.testing.assert_array_equal(h.nsrc, ns)
+    np.testing.assert_array_equal(h.w, w)
+    # one net short: the reader fails as the line reader does
+    q = tmp_path / "short.hgr"
+    body = "".join(lines[:-5])
+    q.write_text(body.replace(f"{g.e + 50} {g.n}", f"{g.e + 56} {g.n}", 1))
+    with pytest.raises(ax.AxcError) as e:
+        ax.read(str(q))
+    assert e.value.code == 5
+
+
 def test_partition_file_roundtrip(tmp_path):
     part = np.array([0, 3, 2, 2, 1], np.uint32)
     p = str(tmp_path / "p.txt")
