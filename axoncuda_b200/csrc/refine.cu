@@ -148,6 +148,82 @@ __global__ void k_census_block(const u32 *__restrict__ list, u32 nlist, CensusAr
     if (threadIdx.x == 0) A.lam[h] = o;
 }
 
+// Partition-indexed census for K <= CD_K: the counters are K-slot arrays indexed by partition id,
+// so a hyperedge of any length fits in shared memory and needs no hashing. Entries are emitted in
+// ascending partition order (the hashed census emits them in order of first occurrence; every
+// consumer reads them as a set). With A.save set, every pin then adds its saving from the count
+// of its own partition.
+constexpr u32 CD_K = 256;
+constexpr u32 CD_WARP_LEN = 1024;  // longer hyperedges take a block
+
+// Counts of hyperedge h's pins over [t0, len) step nt into cnt / dcnt (shared, zeroed).
+__device__ __forceinline__ void cd_count(const CensusArgs &A, u64 a, u64 b, u64 s, u32 *cnt, u32 *dcnt, u32 t0,
+                                         u32 nt) {
+    for (u64 k = a + t0; k < b; k += nt) {
+        const u32 q = A.part[A.pins[k]];
+        atomicAdd(&cnt[q], 1u);
+        if (k >= s) atomicAdd(&dcnt[q], 1u);
+    }
+}
+__device__ __forceinline__ void cd_save(const CensusArgs &A, u32 h, u64 a, u64 b, const u32 *cnt, u32 t0, u32 nt) {
+    if (!A.save) return;
+    const u32 w = A.wfx[h];
+    for (u64 k = a + t0; k < b; k += nt) {
+        const u32 v = A.pins[k];
+        const i64 g = leave_gain(A.encourage, w, cnt[A.part[v]]);
+        if (g) atomicAdd(&A.save[v], (unsigned long long)g);
+    }
+}
+// One warp: the nonzero counters in ascending partition order, then lam.
+__device__ __forceinline__ void cd_emit(const CensusArgs &A, u32 h, u64 a, const u32 *cnt, const u32 *dcnt, u32 K) {
+    const u32 lane = threadIdx.x & 31;
+    u32 o = 0;
+    for (u32 qb = 0; qb < K; qb += 32) {
+        const u32 q = qb + lane;
+        const u32 c = q < K ? cnt[q] : 0;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, c > 0);
+        if (c > 0) {
+            const u64 dst = a + o + __popc(bal & ((1u << lane) - 1u));
+            A.cpart[dst] = q;
+            A.ccnt[dst] = c;
+            A.cdcnt[dst] = dcnt[q];
+        }
+        o += __popc(bal);
+    }
+    if (lane == 0) A.lam[h] = o;
+}
+
+__global__ void k_census_direct_warp(u32 e, CensusArgs A, u32 K) {
+    __shared__ u32 tc[CS_WARPS][CD_K], td[CS_WARPS][CD_K];
+    const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 h = blockIdx.x * CS_WARPS + w;
+    if (h >= e) return;
+    const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+    if (b - a > CD_WARP_LEN) return;
+    u32 *cnt = tc[w], *dcnt = td[w];
+    for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; }
+    __syncwarp();
+    cd_count(A, a, b, s, cnt, dcnt, lane, 32);
+    __syncwarp();
+    cd_save(A, h, a, b, cnt, lane, 32);
+    cd_emit(A, h, a, cnt, dcnt, K);
+}
+
+__global__ void k_census_direct_block(const u32 *__restrict__ list, u32 nlist, CensusArgs A, u32 K) {
+    __shared__ u32 cnt[CD_K], dcnt[CD_K];
+    for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
+        const u32 h = list[idx];
+        const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+        for (u32 i = threadIdx.x; i < K; i += blockDim.x) { cnt[i] = 0; dcnt[i] = 0; }
+        __syncthreads();
+        cd_count(A, a, b, s, cnt, dcnt, threadIdx.x, blockDim.x);
+        __syncthreads();
+        cd_save(A, h, a, b, cnt, threadIdx.x, blockDim.x);
+        if (threadIdx.x < 32) cd_emit(A, h, a, cnt, dcnt, K);
+        __syncthreads();
+    }
+}
+
 __global__ void k_flag_len(u32 e, const u64 *__restrict__ off, u64 lo, u64 hi, u32 *__restrict__ flag) {
     u32 h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h < e) {
@@ -925,7 +1001,7 @@ __device__ __forceinline__ u32 cascade_cap32(u32 lm, u32 m) {
 // target (one shuffle pass over the chunk). The tables are then updated by the whole chunk at once.
 // Equal to the sequential sweep: the counts are exact prefix sums, and transitions are a set.
 __device__ void cascade_sweep_warp(const CascadeArgs &A, u32 h, const u64 *mv, const u32 *sl, u32 m, const u32 *tk,
-                                   u32 *tc, u32 *td) {
+                                   u32 *tc, u32 *td, u32 *lmask) {
     const u32 lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
     const u32 w = A.wfx[h];
     const bool direct = cascade_direct(A);
@@ -937,13 +1013,32 @@ __device__ void cascade_sweep_warp(const CascadeArgs &A, u32 h, const u64 *mv, c
         const u32 sp = act ? (sl[i] & 0xFFFFu) : 0x10000u + lane, sq = act ? (sl[i] >> 16) : 0x20000u + lane;
         const bool dst = act && ((u32)e & MV_DST);
         const u32 dmask = __ballot_sync(0xFFFFFFFFu, dst);
-        const u32 m_pp = __match_any_sync(0xFFFFFFFFu, sp), m_qq = __match_any_sync(0xFFFFFFFFu, sq);
-        u32 m_qp = 0, m_pq = 0;  // lanes whose target is my source / whose source is my target
+        u32 m_pp, m_qq, m_qp = 0, m_pq = 0;  // lanes with my source / my target as source / target
+        if (lmask) {  // direct tables: lmask[x] / lmask[K + x] = lanes with source / target x
+            u32 *pm = lmask, *qm = lmask + A.K;
+            if (act) {
+                atomicOr(&pm[sp], 1u << lane);
+                atomicOr(&qm[sq], 1u << lane);
+            }
+            __syncwarp();
+            m_pp = act ? pm[sp] : 0u;
+            m_qq = act ? qm[sq] : 0u;
+            m_qp = act ? qm[sp] : 0u;
+            m_pq = act ? pm[sq] : 0u;
+            __syncwarp();
+            if (act) {
+                pm[sp] = 0;
+                qm[sq] = 0;
+            }
+        } else {
+            m_pp = __match_any_sync(0xFFFFFFFFu, sp);
+            m_qq = __match_any_sync(0xFFFFFFFFu, sq);
 #pragma unroll 8
-        for (u32 j = 0; j < 32; ++j) {
-            const u32 spj = __shfl_sync(0xFFFFFFFFu, sp, j), sqj = __shfl_sync(0xFFFFFFFFu, sq, j);
-            m_qp |= (u32)(sqj == sp) << j;
-            m_pq |= (u32)(spj == sq) << j;
+            for (u32 j = 0; j < 32; ++j) {
+                const u32 spj = __shfl_sync(0xFFFFFFFFu, sp, j), sqj = __shfl_sync(0xFFFFFFFFu, sq, j);
+                m_qp |= (u32)(sqj == sp) << j;
+                m_pq |= (u32)(spj == sq) << j;
+            }
         }
         const int before_p = __popc(m_qp & lt) - __popc(m_pp & lt);
         const int before_q = __popc(m_qq & lt) - __popc(m_pq & lt);
@@ -1025,14 +1120,17 @@ __global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__rest
     __syncwarp();
     for (u32 i = 0; i < CC_MOV / 32; ++i)
         if (lane + 32 * i < m) mvs[w][posv[i]] = mine[i];
-    // table of partition counts from the census, then the movers' slots
-    for (u32 i = lane; i < cap; i += 32) { tk[w][i] = NONE; tc[w][i] = 0; td[w][i] = 0; }
+    // table of partition counts from the census, then the movers' slots; direct tables leave tk
+    // to the sweep's lane masks (2K <= CC_TAB words, zeroed)
+    for (u32 i = lane; i < cap; i += 32) { tc[w][i] = 0; td[w][i] = 0; }
+    const u32 ntk = direct ? 2 * A.K : cap;
+    for (u32 i = lane; i < ntk; i += 32) tk[w][i] = direct ? 0u : NONE;
     __syncwarp();
     cascade_fill(A, a, lm, tk[w], tc[w], td[w], cap, lane, 32);
     __syncwarp();
     cascade_slots(A, mvs[w], sl[w], m, tk[w], cap, lane, 32);
     __syncwarp();
-    cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w]);
+    cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], direct ? tk[w] : nullptr);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -1060,33 +1158,114 @@ constexpr u32 CB_TAB_HASH = 8192; // hashed table slots of the block kernel, at 
 constexpr size_t CB_DYN_MAX = (size_t)CB_MOV_MAX * 12 + (size_t)CB_TAB_HASH * 12;
 
 // Gather the movers of hyperedge h (rank << 32 | dst flag | node) into mvs[0, min(m, lim)) with
-// the whole block; returns m (all of them, counted past lim). Ends with the block synchronised.
-__device__ __forceinline__ u32 cascade_gather(const CascadeArgs &A, u32 h, u64 *mvs, u32 lim, u32 *cntm) {
+// the whole block; returns m (all of them, counted past lim) and their largest rank in *rmax.
+// Warps reserve their movers' slots with one atomic each. Ends with the block synchronised.
+__device__ __forceinline__ u32 cascade_gather(const CascadeArgs &A, u32 h, u64 *mvs, u32 lim, u32 *cntm, u32 *smax,
+                                              u32 &rmax) {
     const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
-    if (threadIdx.x == 0) *cntm = 0;
+    const u32 lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) { *cntm = 0; *smax = 0; }
     __syncthreads();
-    for (u64 k = a + threadIdx.x; k < b; k += blockDim.x) {
-        const u32 v = A.pins[k], r = A.rank[v];
-        if (r != NONE) {
-            const u32 pos = atomicAdd(cntm, 1u);
+    u32 mymax = 0;
+    for (u64 base = a; base < b; base += blockDim.x) {  // same trip count in every thread
+        const u64 k = base + threadIdx.x;
+        const u32 v = k < b ? A.pins[k] : 0, r = k < b ? A.rank[v] : NONE;
+        const bool mvr = r != NONE;
+        const u32 bal = __ballot_sync(0xFFFFFFFFu, mvr);
+        u32 wbase = 0;
+        if (lane == 0 && bal) wbase = atomicAdd(cntm, (u32)__popc(bal));
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
+        if (mvr) {
+            const u32 pos = wbase + __popc(bal & ((1u << lane) - 1u));
             if (pos < lim) mvs[pos] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
+            mymax = r > mymax ? r : mymax;
         }
     }
+    mymax = __reduce_max_sync(0xFFFFFFFFu, mymax);
+    if (lane == 0 && mymax) atomicMax(smax, mymax);
     __syncthreads();
     const u32 m = *cntm;
-    __syncthreads();  // the count is read before the next hyperedge resets it
+    rmax = *smax;
+    __syncthreads();  // read before the next hyperedge resets them
     return m;
 }
 
-// Sort, tables, slots and sweep of one hyperedge whose m movers are in mvs (block-wide).
-__device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u64 *mvs, u32 *sl, u32 m, u32 *tk,
-                                                  u32 *tc, u32 *td, u32 cap) {
+constexpr u32 CB_SORT_R = 8;                          // keys per thread in the block radix sort
+constexpr u32 CB_RADIX_MAX = CB_SORT_R * CB_THREADS;  // more movers sort bitonically
+
+// Stable LSD radix sort of buf[0, m) (m <= CB_RADIX_MAX, CB_THREADS threads) by key bits
+// [32, 32 + nbits), 2 bits per pass. Thread t holds positions [t*R, t*R + R) in registers; a
+// pass counts its keys' digits in four 16-bit fields of one u64, scans those across the block
+// (warp shuffles plus one shared word per warp) and writes each key to its digit's offset plus
+// the count of equal digits before it. About 30 instructions per key and pass, against the
+// bitonic sort's log^2 m / 2 compare-exchange stages.
+__device__ __forceinline__ void block_radix_sort_hi(u64 *buf, u32 m, u32 nbits, u64 *wsum) {
+    constexpr u32 NW = CB_THREADS / 32;
+    const u32 R = (m + CB_THREADS - 1) / CB_THREADS;
+    const u32 t = threadIdx.x, lane = t & 31, w = t >> 5;
+    u64 key[CB_SORT_R];
+#pragma unroll
+    for (u32 r = 0; r < CB_SORT_R; ++r) {
+        const u32 i = t * R + r;
+        key[r] = (r < R && i < m) ? buf[i] : 0;
+    }
+    for (u32 sh = 0; sh < nbits; sh += 2) {
+        u64 cnt = 0, pre[CB_SORT_R];
+#pragma unroll
+        for (u32 r = 0; r < CB_SORT_R; ++r) {
+            pre[r] = cnt;
+            if (r < R && t * R + r < m) cnt += 1ull << (16 * ((u32)(key[r] >> (32 + sh)) & 3u));
+        }
+        u64 x = cnt;
+#pragma unroll
+        for (u32 o = 1; o < 32; o <<= 1) {
+            const u64 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        u64 wpre = 0, tot = 0;
+#pragma unroll
+        for (u32 i = 0; i < NW; ++i) {
+            if (i < w) wpre += wsum[i];
+            tot += wsum[i];
+        }
+        const u64 excl = wpre + x - cnt;
+        const u32 c0 = (u32)(tot & 0xFFFFu), c1 = (u32)((tot >> 16) & 0xFFFFu), c2 = (u32)((tot >> 32) & 0xFFFFu);
+#pragma unroll
+        for (u32 r = 0; r < CB_SORT_R; ++r) {
+            if (r < R && t * R + r < m) {
+                const u32 d = (u32)(key[r] >> (32 + sh)) & 3u;
+                const u32 off = d == 0 ? 0u : d == 1 ? c0 : d == 2 ? c0 + c1 : c0 + c1 + c2;
+                buf[off + (u32)(((excl + pre[r]) >> (16 * d)) & 0xFFFFu)] = key[r];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (u32 r = 0; r < CB_SORT_R; ++r) {
+            const u32 i = t * R + r;
+            if (r < R && i < m) key[r] = buf[i];
+        }
+    }
+}
+
+// Sort, tables, slots and sweep of one hyperedge whose m movers (largest rank rmax) are in mvs,
+// block-wide. The shared-memory kernel sorts up to CB_RADIX_MAX of them with the block radix sort
+// (wsum set); more, and the scratch kernel's, sort bitonically. Direct tables leave tk to the sweep's lane masks (2K words, zeroed).
+__device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u64 *mvs, u32 *sl, u32 m, u32 rmax,
+                                                  u32 *tk, u32 *tc, u32 *td, u32 cap, u64 *wsum) {
+    const bool direct = cascade_direct(A);
     u32 P = 1;
     while (P < m) P <<= 1;
-    for (u32 i = m + threadIdx.x; i < P; i += blockDim.x) mvs[i] = ~0ull;
-    for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tk[i] = NONE; tc[i] = 0; td[i] = 0; }
+    const bool radix = wsum && m <= CB_RADIX_MAX;
+    if (!radix)
+        for (u32 i = m + threadIdx.x; i < P; i += blockDim.x) mvs[i] = ~0ull;
+    for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { tc[i] = 0; td[i] = 0; }
+    const u32 ntk = direct ? 2 * A.K : cap;
+    for (u32 i = threadIdx.x; i < ntk; i += blockDim.x) tk[i] = direct ? 0u : NONE;
     __syncthreads();
-    block_bitonic_u64(mvs, P);
+    if (radix) block_radix_sort_hi(mvs, m, 32 - __clz(rmax), wsum);
+    else block_bitonic_u64(mvs, P);
     cascade_fill(A, A.off[h], A.lam[h], tk, tc, td, cap, threadIdx.x, blockDim.x);
     __syncthreads();
     if (sl) {
@@ -1094,7 +1273,7 @@ __device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u
         __syncthreads();
     }
     if (sl) {
-        if (threadIdx.x < 32) cascade_sweep_warp(A, h, mvs, sl, m, tk, tc, td);
+        if (threadIdx.x < 32) cascade_sweep_warp(A, h, mvs, sl, m, tk, tc, td, direct ? tk : nullptr);
     } else if (threadIdx.x == 0) {
         cascade_sweep(A, h, mvs, sl, m, tk, tc, td, cap - 1);
     }
@@ -1102,26 +1281,27 @@ __device__ __forceinline__ void cascade_block_one(const CascadeArgs &A, u32 h, u
 }
 
 // Hyperedges with more movers than a warp takes: one block per hyperedge, everything in shared
-// memory (dynamic: smov movers and their slots, then three tables of stab slots). Movers are
-// sorted by rank with a bitonic sort. A hyperedge with more than smov movers, or a hashed table
-// above stab slots, is appended to `huge`.
+// memory (dynamic: smov movers and their slots, then three tables of stab slots). A hyperedge
+// with more than smov movers, or a hashed table above stab slots, is appended to `huge`.
 __global__ void __launch_bounds__(CB_THREADS) k_cascade_block(CascadeArgs A, const u32 *__restrict__ list,
                                                               const u32 *__restrict__ nl, u32 smov, u32 stab,
                                                               u32 *__restrict__ huge, u32 *__restrict__ nhuge) {
     extern __shared__ __align__(16) unsigned char cb_smem[];
-    __shared__ u32 cntm;
+    __shared__ u32 cntm, smax;
+    __shared__ u64 wsum[CB_THREADS / 32];
     u64 *mvs = (u64 *)cb_smem;
     u32 *sl = (u32 *)(mvs + smov), *tk = sl + smov, *tc = tk + stab, *td = tc + stab;
     const bool direct = cascade_direct(A);
     for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
         const u32 h = list[idx];
-        const u32 m = cascade_gather(A, h, mvs, smov, &cntm);
+        u32 rmax;
+        const u32 m = cascade_gather(A, h, mvs, smov, &cntm, &smax, rmax);
         const u32 cap = direct ? A.K : cascade_cap32(A.lam[h], m);
         if (m > smov || cap > stab) {
             if (threadIdx.x == 0) huge[atomicAdd(nhuge, 1u)] = h;
             continue;
         }
-        cascade_block_one(A, h, mvs, sl, m, tk, tc, td, cap);
+        cascade_block_one(A, h, mvs, sl, m, rmax, tk, tc, td, cap, wsum);
     }
 }
 
@@ -1131,17 +1311,18 @@ __global__ void __launch_bounds__(CB_THREADS) k_cascade_huge(CascadeArgs A, cons
                                                              const u32 *__restrict__ nl, u64 *scratch_mv,
                                                              u32 *scratch_sl, u32 *scratch_tab, u64 mv_cap,
                                                              u64 tab_cap) {
-    __shared__ u32 cntm;
+    __shared__ u32 cntm, smax;
     u64 *mvs = scratch_mv + (u64)blockIdx.x * mv_cap;
     u32 *tk = scratch_tab + (u64)blockIdx.x * 3 * tab_cap, *tc = tk + tab_cap, *td = tc + tab_cap;
     const bool direct = cascade_direct(A);
     for (u32 idx = blockIdx.x; idx < *nl; idx += gridDim.x) {
         const u32 h = list[idx];
-        const u32 m = cascade_gather(A, h, mvs, (u32)mv_cap, &cntm);
+        u32 rmax;
+        const u32 m = cascade_gather(A, h, mvs, (u32)mv_cap, &cntm, &smax, rmax);
         const u32 cap = direct ? A.K : cascade_cap32(A.lam[h], m);
         // 16-bit slots cover every direct table and hashed tables of up to 65536 slots
         u32 *sl = (direct || cap <= 65536) ? scratch_sl + (u64)blockIdx.x * mv_cap : nullptr;
-        cascade_block_one(A, h, mvs, sl, m, tk, tc, td, cap);
+        cascade_block_one(A, h, mvs, sl, m, rmax, tk, tc, td, cap, nullptr);
     }
 }
 
@@ -1347,6 +1528,8 @@ struct LevelPrep {
     u64 max_len = 0;         // largest hyperedge
     u64 dst_pins = 0;        // destination pins (bounds the inbound events: 2 per pin)
     u64 tier_deg[3] = {0, 0, 0};  // incidence entries of each gain tier (kernel timer only)
+    u32 census_K = 0;        // nonzero: partition-indexed census over this many partitions, and
+                             // hblock holds the hyperedges above CD_WARP_LEN pins
 };
 
 // Movers the cascade's block kernel keeps in shared memory: CB_MOV_MAX, or less when the
@@ -1398,14 +1581,20 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
     // [6] largest work, [7] largest block-tier work, [8] largest hyperedge, [9] destination pins
     u64 *dc = c.arena.alloc<u64>(10);
     AXC_CUDA(cudaMemsetAsync(dc, 0, 80, c.stream));
+    lp.census_K = K <= CD_K ? K : 0;
     if (e) {
         u32 *flag = c.arena.alloc<u32>(e);
         lp.hblock = c.arena.alloc<u32>(e);
-        lp.hhuge = c.arena.alloc<u32>(e);
-        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
-        compact_indices_dn(c, flag, lp.hblock, e, (u32 *)(dc + 0));
-        LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
-        compact_indices_dn(c, flag, lp.hhuge, e, (u32 *)(dc + 1));
+        if (lp.census_K) {  // partition-indexed census: a warp, or a block above CD_WARP_LEN pins
+            LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CD_WARP_LEN, ~0ull, flag);
+            compact_indices_dn(c, flag, lp.hblock, e, (u32 *)(dc + 0));
+        } else {
+            lp.hhuge = c.arena.alloc<u32>(e);
+            LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_WARP_CAP, (u64)CS_BLOCK_CAP, flag);
+            compact_indices_dn(c, flag, lp.hblock, e, (u32 *)(dc + 0));
+            LAUNCH(c, k_flag_len, cdiv(e, 256), 256, 0, e, L.off, (u64)CS_BLOCK_CAP, ~0ull, flag);
+            compact_indices_dn(c, flag, lp.hhuge, e, (u32 *)(dc + 1));
+        }
         LAUNCH(c, k_level_bounds, cdiv(e, 256), 256, 0, e, L.off, L.nsrc, (unsigned long long *)(dc + 8));
     }
     if (n) {
@@ -1454,6 +1643,12 @@ static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     if (L.e == 0) return;
     CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status,
                  (unsigned long long *)cs.save, cs.wfx, cs.encourage};
+    if (lp.census_K) {
+        LAUNCH(c, k_census_direct_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A, lp.census_K);
+        if (lp.n_hblock)
+            LAUNCH(c, k_census_direct_block, lp.n_hblock, 256, 0, lp.hblock, lp.n_hblock, A, lp.census_K);
+        return;
+    }
     LAUNCH(c, k_census_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A);
     if (lp.n_hblock)
         LAUNCH(c, k_census_block, lp.n_hblock, 256, 4 * 2 * CS_BLOCK_CAP * 4, lp.hblock, lp.n_hblock, A,
@@ -1719,7 +1914,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
             u32 smov = 128;
             while (smov < lp.max_len && smov < cascade_block_movers()) smov <<= 1;
             // hashed tables: sized for the level's largest hyperedge within the block's limit
-            const u32 stab = direct ? std::max(rp.K, 32u)
+            const u32 stab = direct ? std::max(2 * rp.K, 32u)  // tk: the sweep's 2K lane masks
                                     : (u32)std::min<u64>(cascade_cap(std::min<u64>(lp.max_len, rp.K),
                                                                      std::min<u64>(lp.max_len, smov)),
                                                          CB_TAB_HASH);
