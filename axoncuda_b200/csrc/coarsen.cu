@@ -25,6 +25,7 @@ constexpr u32 RT_WARP_W = 256;     // work (incident pins) handled by one warp
 constexpr u32 RT_BLK1_W = 2048;    // block tier 1: table 4096 slots (48 KiB)
 constexpr u32 RT_BLK2_W = 8192;    // block tier 2: table 16384 slots (192 KiB)
 constexpr u32 RT_TRY = 2048;       // first-try table of the block tiers (24 KiB)
+constexpr u32 RT_MID = 8192;       // second try of the larger tier (96 KiB, two blocks per SM)
 constexpr u32 RT_WARPS = 4;
 constexpr u32 RT_BLOCK = 256;
 
@@ -65,7 +66,7 @@ struct RateArgs {
 // With `ndist` set, the table is a first try: distinct keys are counted there, and once they pass
 // `limit` the node stops (the caller retries it with a larger table).
 __device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm, u32 mask, u32 first,
-                          u32 stride, u32 *ndist = nullptr, u32 limit = 0) {
+                          u32 stride, u32 *ndist = nullptr, u32 limit = 0, u32 *used = nullptr) {
     const u32 lane = threadIdx.x & 31u;
     const u64 t0 = A.toff[u];
     const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
@@ -104,12 +105,20 @@ __device__ void rate_flat(const RateArgs &A, u32 u, u32 *keys, u32 *sc, u32 *cm,
             const u32 v = A.pins[ao + i];
             if (v == u) continue;
             u32 slot;
-            if (ndist) {  // bounded table: count distinct keys, give up past `limit`
+            if (ndist) {  // counted keys: a first try gives up past `limit`; `used` lists them
                 if (*(volatile u32 *)ndist > limit) continue;
                 bool fresh = false;
                 slot = hash_insert_fresh(keys, mask, v, fresh);
-                if (fresh && atomicAdd(ndist, 1u) + 1 > limit) continue;
-                if (slot == NONE) { atomicExch(ndist, limit + 1); continue; }
+                if (slot == NONE) {  // full: a first try overflows, a sized table is an error
+                    if (used) atomicExch(A.status, DEV_HASH_FULL);
+                    else atomicExch(ndist, limit + 1);
+                    continue;
+                }
+                if (fresh) {
+                    const u32 idx = atomicAdd(ndist, 1u);
+                    if (used) used[idx] = slot;
+                    if (idx + 1 > limit) continue;
+                }
             } else {
                 slot = hash_find_or_insert(keys, mask, v);
                 if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
@@ -141,13 +150,16 @@ __device__ __forceinline__ void top_insert(u64 (&top)[AXC_MAX_CANDIDATES], u64 k
             k = t;
         }
 }
+// Slots [first, cap) step `step` of the table, or with `used` the listed slots used[first, cap).
 __device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm,
-                                           u32 cap, u32 first, u32 step, u64 (&top)[AXC_MAX_CANDIDATES]) {
+                                           u32 cap, u32 first, u32 step, u64 (&top)[AXC_MAX_CANDIDATES],
+                                           const u32 *used = nullptr) {
 #pragma unroll
     for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i) top[i] = 0;
     const u32 cnc = A.cnc;
     u64 floor = 0;  // the list's last entry: a key must beat it to enter
-    for (u32 s = first; s < cap; s += step) {
+    for (u32 t = first; t < cap; t += step) {
+        const u32 s = used ? used[t] : t;
         const u32 v = keys[s];
         if (v == NONE) continue;
         const u64 k = cand_key(A, u, v, sc[s], cm[s]);
@@ -195,11 +207,12 @@ constexpr u32 RT_SEL = (RT_BLOCK / 32) * AXC_MAX_CANDIDATES;  // shared slots of
 // The top-cnc candidates of node u from its table (keys, sc, cm) of `cap` slots; block-wide.
 // Each warp reduces its lanes' lists to its own top cnc with shuffles into red[warp * cnc ..];
 // warp 0 merges those after one barrier. red holds RT_SEL entries.
+// With `used`, only the nused listed slots are read.
 __device__ void rate_select(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm, u32 cap,
-                            u64 *red) {
+                            u64 *red, const u32 *used = nullptr, u32 nused = 0) {
     const u32 lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5, cnc = A.cnc;
     u64 top[AXC_MAX_CANDIDATES];
-    top_collect(A, u, keys, sc, cm, cap, threadIdx.x, blockDim.x, top);
+    top_collect(A, u, keys, sc, cm, used ? nused : cap, threadIdx.x, blockDim.x, top, used);
     for (u32 r = 0; r < cnc; ++r) {
         const u64 best = warp_max_u64(top[0]);
         if (lane == 0) red[w * cnc + r] = best;
@@ -245,42 +258,61 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, cons
 }
 
 // One node per block iteration; table in dynamic smem (gtab == nullptr) or in this block's
-// slice of a global scratch region.
+// slice of a global scratch region. A global slice (keys | sc | cm planes of cap_max slots) is
+// emptied once at the start; each node lists the slots it fills in its slice of gused, reads its
+// candidates from those and empties them again, so its cost follows its distinct neighbours,
+// not the slice size.
 // With `retry` set the launch is a first try on tables smaller than the nodes' work bounds: a node
 // whose distinct neighbours pass half of its table stops and is appended to retry / *d_retry.
 // With `d_nl` set the list length is read from device memory (at most nlist).
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
                                                         u32 cap_max, u32 *gtab, const u32 *__restrict__ d_nl,
-                                                        u32 *__restrict__ retry, u32 *__restrict__ d_retry) {
+                                                        u32 *__restrict__ retry, u32 *__restrict__ d_retry,
+                                                        u32 *gused) {
     extern __shared__ u32 dyn[];
     __shared__ u64 red[RT_SEL];
     __shared__ u32 ndist;
-    u32 *keys, *sc, *cm;
+    u32 *keys, *sc, *cm, *used = nullptr;
+    if (d_nl) nlist = min(nlist, *d_nl);
     if (gtab) {
         keys = gtab + (u64)blockIdx.x * 3 * cap_max;
+        sc = keys + cap_max;
+        cm = sc + cap_max;
+        used = gused + (u64)blockIdx.x * cap_max;
+        if (blockIdx.x < nlist)
+            for (u32 i = threadIdx.x; i < cap_max; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
     } else {
         keys = dyn;
     }
-    if (d_nl) nlist = min(nlist, *d_nl);
     for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
         const u32 u = list[idx];
         // table size from the node's work bound, capped by the node count
         const u64 W = A.work[u] < A.n ? A.work[u] : A.n;
         u32 cap = 64;
         while (cap < 2 * W && cap < cap_max) cap <<= 1;
-        sc = keys + cap;
-        cm = sc + cap;
-        for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
+        if (!gtab) {
+            sc = keys + cap;
+            cm = sc + cap;
+            for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; sc[i] = 0; cm[i] = 0; }
+        }
         if (threadIdx.x == 0) ndist = 0;
         __syncthreads();
-        const u32 limit = cap / 2;
-        rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x, retry ? &ndist : nullptr,
-                  limit);
+        const u32 limit = gtab ? cap : cap / 2;
+        rate_flat(A, u, keys, sc, cm, cap - 1, 32 * (threadIdx.x >> 5), blockDim.x,
+                  (retry || gtab) ? &ndist : nullptr, limit, used);
         __syncthreads();
         if (retry && ndist > limit) {  // table too small: the retry launch redoes this node
             if (threadIdx.x == 0) retry[atomicAdd(d_retry, 1u)] = u;
         } else {
-            rate_select(A, u, keys, sc, cm, cap, red);
+            rate_select(A, u, keys, sc, cm, cap, red, used, ndist);
+        }
+        if (gtab) {  // rate_select ends with a barrier: empty the listed slots
+            for (u32 t = threadIdx.x; t < ndist; t += blockDim.x) {
+                const u32 s2 = used[t];
+                keys[s2] = NONE;
+                sc[s2] = 0;
+                cm[s2] = 0;
+            }
         }
         __syncthreads();
     }
@@ -553,20 +585,30 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     // Nodes' work bounds count pins with multiplicity; their distinct neighbours are usually far
     // fewer. A first launch tries RT_TRY-slot tables (more blocks per SM); nodes that outgrow
     // theirs are redone by a second launch with the tier's full tables.
-    u32 *retry = c.arena.alloc<u32>(n), *d_retry = (u32 *)(dc + 4);  // dc[4] was read already
+    // A node that outgrows an RT_TRY table retries at RT_MID slots (two blocks per SM) when the
+    // tier's tables are larger still, and only past that at the tier's full size.
+    u32 *retry = c.arena.alloc<u32>(n), *retry2 = c.arena.alloc<u32>(n);
+    u32 *d_retry = (u32 *)(dc + 4), *d_retry2 = d_retry + 1;  // dc[4] was read already
     auto block_tier = [&](const u32 *lst, u32 cnt, u32 cap_full) {
         if (!cnt) return;
         if (cap_full <= RT_TRY) {
             LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * cap_full * 4, A, lst, cnt, cap_full, (u32 *)nullptr,
-                   (const u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
+                   (const u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
             return;
         }
-        AXC_CUDA(cudaMemsetAsync(d_retry, 0, 4, c.stream));
+        AXC_CUDA(cudaMemsetAsync(d_retry, 0, 8, c.stream));  // d_retry and d_retry2
         LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * RT_TRY * 4, A, lst, cnt, RT_TRY, (u32 *)nullptr,
-               (const u32 *)nullptr, retry, d_retry);
+               (const u32 *)nullptr, retry, d_retry, (u32 *)nullptr);
+        const u32 *rl = retry, *dn = d_retry;
+        if (cap_full > RT_MID) {
+            LAUNCH(c, k_rate_block, std::min<u32>(cnt, (u32)c.sms * 2), RT_BLOCK, 3 * RT_MID * 4, A, rl, cnt, RT_MID,
+                   (u32 *)nullptr, dn, retry2, d_retry2, (u32 *)nullptr);
+            rl = retry2;
+            dn = d_retry2;
+        }
         const u32 grid = std::min<u32>(cnt, (u32)c.sms * 2);
-        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 3 * cap_full * 4, A, (const u32 *)retry, cnt, cap_full,
-               (u32 *)nullptr, (const u32 *)d_retry, (u32 *)nullptr, (u32 *)nullptr);
+        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 3 * cap_full * 4, A, rl, cnt, cap_full, (u32 *)nullptr, dn,
+               (u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
     };
     block_tier(list2, nl, cap1);
     // tier: one block per node, up to 16384-slot table in dynamic smem
@@ -590,10 +632,10 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
             LAUNCH(c, k_rate_split_select, nl, RT_BLOCK, 0, A, list4, nl, cap, gtab);
         } else {
             u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
-            u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap);
+            u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap), *gused = c.arena.alloc<u32>((u64)grid * cap);
             if (c.profiling("k_rate_block")) c.prof_bytes += 4 * tier_visits[2] + 8ull * cnc * nl;
             LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab, (const u32 *)nullptr, (u32 *)nullptr,
-                   (u32 *)nullptr);
+                   (u32 *)nullptr, gused);
         }
     }
     check_status(c);

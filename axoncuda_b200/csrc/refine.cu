@@ -46,6 +46,10 @@ struct CensusArgs {
     unsigned long long *save;
     const u32 *wfx;
     int encourage;
+    // partition-indexed census only, when set: the hyperedge's masks of partitions present and
+    // with destination pins, mw words each
+    u32 *mask, *dmask;
+    u32 mw;
 };
 
 // insert phase: keys = partition, mn = first position, cnt/dcnt counters
@@ -174,14 +178,23 @@ __device__ __forceinline__ void cd_save(const CensusArgs &A, u32 h, u64 a, u64 b
         if (g) atomicAdd(&A.save[v], (unsigned long long)g);
     }
 }
-// One warp: the nonzero counters in ascending partition order, then lam.
+// One warp: the nonzero counters in ascending partition order, then lam. The ballots of the
+// counters are the hyperedge's masks, written when A.mask is set.
 __device__ __forceinline__ void cd_emit(const CensusArgs &A, u32 h, u64 a, const u32 *cnt, const u32 *dcnt, u32 K) {
     const u32 lane = threadIdx.x & 31;
     u32 o = 0;
-    for (u32 qb = 0; qb < K; qb += 32) {
+    const u32 qend = A.mask ? 32 * A.mw : K;
+    for (u32 qb = 0; qb < qend; qb += 32) {
         const u32 q = qb + lane;
         const u32 c = q < K ? cnt[q] : 0;
         const u32 bal = __ballot_sync(0xFFFFFFFFu, c > 0);
+        if (A.mask) {
+            const u32 dbal = __ballot_sync(0xFFFFFFFFu, c > 0 && dcnt[q] > 0);
+            if (lane == 0) {
+                A.mask[(u64)h * A.mw + qb / 32] = bal;
+                A.dmask[(u64)h * A.mw + qb / 32] = dbal;
+            }
+        }
         if (c > 0) {
             const u64 dst = a + o + __popc(bal & ((1u << lane) - 1u));
             A.cpart[dst] = q;
@@ -854,9 +867,13 @@ __global__ void k_tier(u32 n, u32 K, const u64 *__restrict__ work, const u64 *__
 }
 
 // ------------------------------------------------------------------ ranking
-__global__ void k_move_flags(u32 n, const u32 *__restrict__ target, u32 *__restrict__ flag) {
+// Mover flags, and every node's rank reset (k_set_rank then ranks the movers).
+__global__ void k_move_flags(u32 n, const u32 *__restrict__ target, u32 *__restrict__ flag, u32 *__restrict__ rank) {
     u32 v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n) flag[v] = target[v] != NONE ? 1u : 0u;
+    if (v < n) {
+        flag[v] = target[v] != NONE ? 1u : 0u;
+        rank[v] = NONE;
+    }
 }
 __global__ void k_move_keys(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const i64 *__restrict__ gain,
                             u64 gbound, u32 *__restrict__ hi, u32 *__restrict__ lo) {
@@ -1327,10 +1344,16 @@ __global__ void __launch_bounds__(CB_THREADS) k_cascade_huge(CascadeArgs A, cons
 }
 
 // ------------------------------------------------------------------ prefix and validity
+// G[i] = the cascaded gain of the i-th mover; the two following nmax-entry blocks (the size and
+// inbound violations) start at zero.
 __global__ void k_gather_g2(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 nmax,
                             const unsigned long long *__restrict__ g2, i64 *__restrict__ G) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nmax) G[i] = i < *dM ? (i64)g2[mv[i]] : 0;
+    if (i < nmax) {
+        G[i] = i < *dM ? (i64)g2[mv[i]] : 0;
+        G[(u64)nmax + i] = 0;
+        G[2 * (u64)nmax + i] = 0;
+    }
 }
 
 // size events: 2r = leave p, 2r+1 = join q
@@ -1642,8 +1665,11 @@ static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     cs.beg = L.off;
     if (L.e == 0) return;
     CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status,
-                 (unsigned long long *)cs.save, cs.wfx, cs.encourage};
+                 (unsigned long long *)cs.save, cs.wfx, cs.encourage, nullptr, nullptr, 0};
     if (lp.census_K) {
+        A.mask = cs.mask;  // masks come with the partition-indexed census
+        A.dmask = cs.dmask;
+        A.mw = cs.mw;
         LAUNCH(c, k_census_direct_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A, lp.census_K);
         if (lp.n_hblock)
             LAUNCH(c, k_census_direct_block, lp.n_hblock, 256, 0, lp.hblock, lp.n_hblock, A, lp.census_K);
@@ -1697,8 +1723,7 @@ static void run_gains_masked(Ctx &c, const LevelPrep &lp, const GainArgs &A, con
 }
 
 static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainArgs &A, const Census &cs) {
-    fill_u32(c, A.target, NONE, L.n);
-    if (cs.mask) {  // partition-indexed gains (K <= GN_DIRECT_K)
+    if (cs.mask) {  // partition-indexed gains (K <= GN_DIRECT_K); their two tiers write every node
         if (c.profiling("k_gain_mask_warp")) c.prof_bytes += gain_bytes(lp, 0);
         if (c.profiling("k_gain_mask_block")) c.prof_bytes += gain_bytes(lp, 1);
         switch (cs.mw) {
@@ -1709,6 +1734,7 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
         }
         return;
     }
+    fill_u32(c, A.target, NONE, L.n);
     if (c.profiling("k_gain_warp") && lp.ncount[0]) c.prof_bytes += gain_bytes(lp, 0);
     if (c.profiling("k_gain_block")) c.prof_bytes += gain_bytes(lp, 1) + gain_bytes(lp, 2);
     LAUNCH(c, k_gain_warp, cdiv(lp.ncount[0], GN_WARPS), GN_WARPS * 32, 0, A, lp.ntier[0], lp.ncount[0], lp.work);
@@ -1811,15 +1837,15 @@ static Census census_for_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, con
         cs.wfx = wfx;
         cs.encourage = rp.encourage ? 1 : 0;
     }
-    run_census(c, L, lp, part, cs);
     if (direct) {
         cs.mw = mask_words(rp.K);
         cs.mask = c.arena.alloc<u32>((u64)(L.e ? L.e : 1) * cs.mw);
         cs.dmask = c.arena.alloc<u32>((u64)(L.e ? L.e : 1) * cs.mw);
-        if (L.e)
-            LAUNCH(c, k_census_masks, cdiv((u64)L.e * 32, 256), 256, 0, L.e, L.off, cs.lam, cs.part, cs.dcnt, cs.mw,
-                   cs.mask, cs.dmask);
     }
+    run_census(c, L, lp, part, cs);
+    if (direct && L.e && !lp.census_K)  // a hashed census: masks from its entries
+        LAUNCH(c, k_census_masks, cdiv((u64)L.e * 32, 256), 256, 0, L.e, L.off, cs.lam, cs.part, cs.dcnt, cs.mw,
+               cs.mask, cs.dmask);
     return cs;
 }
 
@@ -1865,8 +1891,8 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
     u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4;
     // movers in id order, then ranked by (gain desc, id asc)
-    u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag);
+    u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n), *rank = c.arena.alloc<u32>(n);
+    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag, rank);
     compact_indices_dn(c, flag, mv, n, dM);
     const u32 kb = bits_for(lp.gain_bound);
     u32 *khi = c.arena.alloc<u32>(n), *klo = c.arena.alloc<u32>(n);
@@ -1881,8 +1907,6 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     } else {
         radix_sort_pairs_dn(c, klo, mv, dM, n, kb);
     }
-    u32 *rank = flag;
-    fill_u32(c, rank, NONE, n);
     LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank);
     // cascade
     unsigned long long *g2 = c.arena.alloc<unsigned long long>(n);
@@ -1944,8 +1968,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     // one buffer [G | Vs | Vi] so one inclusive scan makes all three prefix sums
     i64 *raw = c.arena.alloc<i64>(3 * (u64)n), *pre = c.arena.alloc<i64>(3 * (u64)n);
     i64 *Gx = raw, *Vs = raw + n, *Vi = raw + 2 * (u64)n;
-    LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);
-    AXC_CUDA(cudaMemsetAsync(Vs, 0, (size_t)n * 16, c.stream));  // Vs and Vi
+    LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);  // also zeroes Vs and Vi
     // size validity
     {
         size_t m1 = c.arena.mark();

@@ -85,6 +85,28 @@ def test_rating_matches_oracle(ctx, name, size, omega, delta, cnc):
     np.testing.assert_array_equal(scores, o_scores)
 
 
+def random_hyperedges(n, e, size, seed):
+    """e hyperedges of `size` distinct uniform pins (the first one the source): neighbourhoods
+    with almost no repeats, so nodes' distinct neighbours come close to their work bounds."""
+    rng = np.random.default_rng(seed)
+    pins = np.concatenate([rng.choice(n, size, replace=False) for _ in range(e)]).astype(np.uint32)
+    off = np.arange(e + 1, dtype=np.uint64) * size
+    return ax.Hypergraph(n, off, pins, np.ones(e, np.uint32), np.ones(e, np.float32))
+
+
+# Rating tables: nodes whose distinct neighbours outgrow the first try (2048 slots) retry at
+# 8192 slots, then at the tier's full size (about 40 hyperedges of 100 pins per node); nodes above
+# 8192 pin visits use global tables whose filled slots are listed (about 100 per node).
+@pytest.mark.parametrize("e", [8000, 20000])
+def test_rating_retries_and_global_tables_match_oracle(ctx, e):
+    g = random_hyperedges(20000, e, 100, e)
+    ns = np.ones(g.n, np.uint32)
+    pairs, scores = ctx.stage_rating(g, ns, 1 << 20, 1 << 20, 4)
+    o_pairs, o_scores = O.rating(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, 1 << 20, 1 << 20, 4)
+    np.testing.assert_array_equal(pairs, o_pairs)
+    np.testing.assert_array_equal(scores, o_scores)
+
+
 @pytest.mark.parametrize("wl", ["snn-8x512", "circuit-200k-k2"])
 def test_rating_full_size(ctx, wl):
     g, p = ax.workload(wl)
