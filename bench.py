@@ -149,6 +149,8 @@ BYTE_MODELS = {
     "k_rate_block": "4 B per pin visit of the listed nodes (the pin id) + 8 B per candidate slot written",
     "k_gain_warp": "8 B per incidence entry of the listed nodes + 16 B per listed node",
     "k_gain_block": "8 B per incidence entry of the listed nodes + 16 B per listed node",
+    "k_gain_mask_warp": "8 B per incidence entry of the listed nodes + 16 B per listed node",
+    "k_gain_mask_block": "8 B per incidence entry of the listed nodes + 16 B per listed node",
 }
 
 
