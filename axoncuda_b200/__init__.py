@@ -77,6 +77,7 @@ EXPORTS = [
     "axc_params_preset", "axc_kway_omega", "axc_partition", "axc_partition_device", "axc_evaluate",
     "axc_read_hgr", "axc_read_snn", "axc_read_axh", "axc_read_auto", "axc_free_hgraph",
     "axc_write_hgraph", "axc_write_partition", "axc_read_partition", "axc_quotient_hgraph",
+    "axc_quotient_hgraph_device",
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
     "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
@@ -115,6 +116,7 @@ def lib() -> C.CDLL:
             "axc_write_partition": (C.c_int, [C.c_char_p, u32p, C.c_uint32]),
             "axc_read_partition": (C.c_int, [C.c_char_p, C.c_uint32, u32p]),
             "axc_quotient_hgraph": (C.c_int, [H, u32p, H]),
+            "axc_quotient_hgraph_device": (C.c_int, [C.c_void_p, H, u32p, H]),
             "axc_gen_snn": (C.c_int, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32,
                                       C.c_double, C.c_uint64, H]),
             "axc_gen_circuit": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
@@ -297,6 +299,17 @@ class Context:
         self._check(lib().axc_evaluate(self._h, C.byref(g.c()), C.byref(p), _ptr(part, C.c_uint32),
                                        C.byref(st)), "axc_evaluate")
         return st
+
+    def quotient(self, g: Hypergraph, part: np.ndarray) -> Hypergraph:
+        """The quotient hypergraph written by `-s` (axc_quotient_hgraph_device)."""
+        part = np.ascontiguousarray(part, dtype=np.uint32)
+        q = HGraph()
+        self._check(lib().axc_quotient_hgraph_device(self._h, C.byref(g.c()), _ptr(part, C.c_uint32), C.byref(q)),
+                    "axc_quotient_hgraph_device")
+        try:
+            return Hypergraph.from_c(q)
+        finally:
+            lib().axc_free_hgraph(C.byref(q))
 
     def submit(self, g: Hypergraph, p: Params) -> int:
         jid = C.c_uint64()

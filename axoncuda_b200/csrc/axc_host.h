@@ -19,6 +19,14 @@ struct HostGraph {
 
 void publish(HostGraph *hg, axc_hgraph *out);
 
+// The quotient hypergraph from per-hyperedge partition lists: qcnt[h] kept partitions of
+// hyperedge h (0: the hyperedge vanishes), the first qsrc[h] of them its sources, all in qpins
+// in hyperedge order. Identical (sources, destinations) pairs merge with their weights summed in
+// hyperedge order (1 each when w is null); the result lists them in ascending lexicographic
+// order of (sources, destinations) over K nodes.
+HostGraph *quotient_merge(uint32_t K, uint32_t e, const std::vector<uint32_t> &qcnt, const std::vector<uint32_t> &qsrc,
+                          const std::vector<uint32_t> &qpins, const float *w);
+
 // Lanes of the batching / serving executor (driver.cu): a stream, status word and scan state of
 // their own; each job runs in a fresh device arena of the size the executor grants it.
 struct Lane;

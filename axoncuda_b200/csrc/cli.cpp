@@ -133,7 +133,11 @@ int main(int argc, char **argv) {
     }
     axc_hgraph q;
     std::memset(&q, 0, sizeof q);
-    axc_quotient_hgraph(&g, part.data(), &q);
+    rc = axc_quotient_hgraph_device(ctx, &g, part.data(), &q);
+    if (rc) {
+        std::fprintf(stderr, "quotient hypergraph failed: %s (%s)\n", axc_strerror(rc), axc_last_error(ctx));
+        return 1;
+    }
     const uint64_t qP = q.e ? q.hedge_off[q.e] : 0;
     std::printf("Partitioned hypergraph:\n");
     std::printf("  Nodes:         %u\n", st.num_parts);

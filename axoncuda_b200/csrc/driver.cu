@@ -649,6 +649,31 @@ int axc_evaluate(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, const u
     }
 }
 
+int axc_quotient_hgraph_device(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, axc_hgraph *out) {
+    if (!ctx || check_graph(g) || !out || (!part && g->n)) return AXC_EINVAL;
+    uint32_t K = 0;
+    for (uint32_t v = 0; v < g->n; ++v) K = std::max(K, part[v] + 1);
+    if (g->n && K == 0) return AXC_EOVERFLOW;  // an id of 2^32 - 1
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Ctx &c = ctx->c;
+    try {
+        const size_t m = c.arena.mark();
+        u64 P = 0;
+        axc_hgraph d = upload(c, g, P);
+        u32 *dp = c.arena.alloc<u32>(g->n ? g->n : 1);
+        if (g->n) AXC_CUDA(cudaMemcpyAsync(dp, part, (size_t)g->n * 4, cudaMemcpyHostToDevice, c.stream));
+        std::vector<u32> qcnt, qsrc, qpins;
+        quotient_extract(c, g->e, P, d.hedge_off, d.pins, d.src_count, dp, K, qcnt, qsrc, qpins);
+        c.arena.release(m);
+        publish(quotient_merge(K, g->e, qcnt, qsrc, qpins, g->hedge_w), out);
+        return AXC_OK;
+    } catch (const std::exception &e) {
+        cudaStreamSynchronize(c.stream);
+        c.arena.release(0);
+        return guard(ctx, e);
+    }
+}
+
 // ---------------------------------------------------------------- stage entry points
 int axc_stage_construct(axc_ctx *ctx, const axc_hgraph *g, uint64_t *out_hedge_off, uint32_t *out_pins,
                         uint32_t *out_src_count, uint64_t *out_touch_off, uint32_t *out_touch, uint32_t *out_inbound,

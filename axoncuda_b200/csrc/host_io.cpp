@@ -412,6 +412,51 @@ extern "C" int axc_read_partition(const char *path, uint32_t n, uint32_t *out) {
     return idx == n ? AXC_OK : AXC_EFORMAT;
 }
 
+namespace axc {
+
+HostGraph *quotient_merge(uint32_t K, uint32_t e, const std::vector<uint32_t> &qcnt, const std::vector<uint32_t> &qsrc,
+                          const std::vector<uint32_t> &qpins, const float *w) {
+    struct Item {
+        uint64_t at;  // first entry in qpins
+        uint32_t ns, nd, h;
+    };
+    std::vector<Item> items;
+    uint64_t at = 0;
+    for (uint32_t h = 0; h < e; ++h) {
+        if (!qcnt[h]) continue;
+        items.push_back({at, qsrc[h], qcnt[h] - qsrc[h], h});
+        at += qcnt[h];
+    }
+    const uint32_t *q = qpins.data();
+    auto less = [&](const Item &x, const Item &y) {  // std::pair<std::vector, std::vector> order
+        const uint32_t *xs = q + x.at, *ys = q + y.at;
+        if (std::lexicographical_compare(xs, xs + x.ns, ys, ys + y.ns)) return true;
+        if (std::lexicographical_compare(ys, ys + y.ns, xs, xs + x.ns)) return false;
+        return std::lexicographical_compare(xs + x.ns, xs + x.ns + x.nd, ys + y.ns, ys + y.ns + y.nd);
+    };
+    auto same = [&](const Item &x, const Item &y) {
+        return x.ns == y.ns && x.nd == y.nd && std::equal(q + x.at, q + x.at + x.ns + x.nd, q + y.at);
+    };
+    std::stable_sort(items.begin(), items.end(), less);  // equal keys stay in hyperedge order
+    auto *hg = new HostGraph();
+    hg->n = K;
+    hg->off.push_back(0);
+    for (size_t i = 0; i < items.size();) {
+        size_t j = i;
+        double sum = 0.0;
+        for (; j < items.size() && same(items[i], items[j]); ++j) sum += w ? (double)w[items[j].h] : 1.0;
+        const Item &it = items[i];
+        hg->pins.insert(hg->pins.end(), q + it.at, q + it.at + it.ns + it.nd);
+        hg->nsrc.push_back(it.ns);
+        hg->w.push_back((float)sum);
+        hg->off.push_back(hg->pins.size());
+        i = j;
+    }
+    return hg;
+}
+
+}  // namespace axc
+
 // Quotient hypergraph of getPartitionsHypergraph(part, remove_self_cycles=2, squish=true)
 // (includes/hgraph.hpp:286-376): per hedge the distinct source partitions and the distinct
 // destination partitions minus the source ones; hedges with <= 1 source partition and no

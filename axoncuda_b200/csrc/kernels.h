@@ -87,6 +87,10 @@ void merge_small_partitions(Ctx &c, const DLevel &L, u32 *part, u32 K, u32 omega
 // zero-base partition ids in order of old id; returns K'
 u32 zero_base(Ctx &c, u32 n, u32 *part, u32 K);
 // metrics over a level graph (any graph as given): fills the fx fields of stats
+// quotient.cu: the distinct source / destination-only partitions of every hyperedge (device
+// input, host output; see axc_quotient_hgraph_device)
+void quotient_extract(Ctx &c, u32 e, u64 P, const u64 *off, const u32 *pins, const u32 *nsrc, const u32 *part, u32 K,
+                      std::vector<u32> &qcnt, std::vector<u32> &qsrc, std::vector<u32> &qpins);
 void evaluate(Ctx &c, const DLevel &L, const u32 *wfx, const u32 *part, u32 omega, u32 delta,
               u32 max_parts, axc_stats *st);
 

@@ -181,6 +181,12 @@ int axc_read_partition(const char *path, uint32_t n, uint32_t *out);
 /* getPartitionsHypergraph(part, 2, squish=true) (includes/hgraph.hpp:286-376): the quotient
  * hypergraph written by `-s`; identical (source set, destination set) hyperedges are merged. */
 int axc_quotient_hgraph(const axc_hgraph *g, const uint32_t *part, axc_hgraph *out);
+/* The same quotient hypergraph with the per-hyperedge work on the context's GPU: one radix sort
+ * of (hyperedge, side, partition) keys over all pins; only the distinct partitions come back to
+ * the host, which merges identical pairs. The output equals axc_quotient_hgraph's. Partition ids
+ * must be below 2^31 and the pins fewer than 2^32 (else AXC_EOVERFLOW). Free `out` with
+ * axc_free_hgraph. */
+int axc_quotient_hgraph_device(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, axc_hgraph *out);
 
 /* ---- synthetic inputs (seeded; stand-ins for the public SNN / ISPD suites) -----------------------
  * Layered SNN: `layers` x `width` neurons; every neuron of layers 0..layers-2 owns one hyperedge

@@ -300,6 +300,43 @@ def test_partition_full_size_matches_oracle(ctx, wl):
     assert ev["connectivity_fx"] == st.connectivity_fx
 
 
+def host_quotient(g, part):
+    import ctypes as C
+    q = ax.HGraph()
+    assert ax.lib().axc_quotient_hgraph(C.byref(g.c()), part.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(q)) == 0
+    try:
+        return ax.Hypergraph.from_c(q)
+    finally:
+        ax.lib().axc_free_hgraph(C.byref(q))
+
+
+# The `-s` quotient hypergraph on the device must equal the host construction exactly: nodes,
+# hyperedge order, source / destination lists and merged weights. Cases: SNN hyperedges with
+# sources, hMETIS nets without, duplicate pins, one partition, many partitions, weights.
+@pytest.mark.parametrize("name,K", [("snn_4x64.snn", 7), ("circ_2k.hgr", 40), ("tiny_dups.hgr", 3),
+                                    ("snn_5x40_ln.snn", 1), ("tiny_w.hgr", 2), ("snn_4x64.snn", 256)])
+def test_device_quotient_matches_host(ctx, name, K):
+    g = golden(name)
+    rng = np.random.default_rng(K)
+    part = rng.integers(0, K, g.n).astype(np.uint32)
+    q = ctx.quotient(g, part)
+    h = host_quotient(g, part)
+    assert q.n == h.n
+    np.testing.assert_array_equal(q.off, h.off)
+    np.testing.assert_array_equal(q.pins, h.pins)
+    np.testing.assert_array_equal(q.nsrc, h.nsrc)
+    np.testing.assert_array_equal(q.w, h.w)
+
+
+def test_device_quotient_of_a_partition(ctx):
+    g, p = ax.workload("snn-8x512")
+    part, st = ctx.partition(g, p)
+    q, h = ctx.quotient(g, part), host_quotient(g, part)
+    assert q.n == st.num_parts and q.e == h.e
+    np.testing.assert_array_equal(q.pins, h.pins)
+    np.testing.assert_array_equal(q.w, h.w)
+
+
 def test_evaluate_matches_oracle(ctx):
     g = golden("circ_2k.hgr")
     rng = np.random.default_rng(5)
