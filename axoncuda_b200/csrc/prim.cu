@@ -184,13 +184,17 @@ __device__ TO lookback_prefix(const ScanState &S, u32 epoch, u32 t, TO tile_tota
 }
 
 // Scan: out[i] = sum of in[0..i) (exclusive) or in[0..i] (inclusive), in one pass.
+// With skip_n set, a launch whose *skip_n is at most skip_le does nothing: every block returns
+// before it takes a tile ticket, so the tile state is left as the previous launch left it.
 template <class TI, class TO, bool INCL>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_lb(const TI *__restrict__ in, TO *__restrict__ out, u64 n,
-                                                        ScanState S, u32 *status) {
+                                                        ScanState S, u32 *status, const u32 *__restrict__ skip_n,
+                                                        u32 skip_le) {
     __shared__ TO wt[33];
     __shared__ TO stage[SCAN_TILE + SCAN_TILE / 32];
     __shared__ u32 s_tile, s_epoch;
     __shared__ TO s_prefix;
+    if (skip_n && *skip_n <= skip_le) return;
     u32 epoch;
     const u32 t = lb_enter(S, s_tile, s_epoch, epoch);
     const u64 base = (u64)t * SCAN_TILE;
@@ -257,11 +261,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_compact_lb(const u32 *__restri
 }
 
 template <class TI, class TO, bool INCL = false>
-void scan_impl(Ctx &c, const TI *in, TO *out, u64 n) {
+void scan_impl(Ctx &c, const TI *in, TO *out, u64 n, const u32 *skip_n = nullptr, u32 skip_le = 0) {
     if (n == 0) return;
     const u32 tiles = cdiv(n, SCAN_TILE);
     if (tiles <= c.scan.cap_tiles) {
-        LAUNCH(c, (k_scan_lb<TI, TO, INCL>), tiles, SCAN_THREADS, 0, in, out, n, c.scan, c.d_status);
+        LAUNCH(c, (k_scan_lb<TI, TO, INCL>), tiles, SCAN_THREADS, 0, in, out, n, c.scan, c.d_status, skip_n, skip_le);
         return;
     }
     if (INCL) throw Error(AXC_EOVERFLOW, "inclusive scan longer than the look-back tile state");
@@ -286,8 +290,11 @@ constexpr int RS_WARPS = 8;
 constexpr int RS_ITEMS = 8;  // rounds of 32 per warp
 constexpr int RS_TILE = RS_WARPS * 32 * RS_ITEMS;
 
+// k_rs_hist / k_rs_scatter: with d_n set, a count of at most skip_le means the one-block sort
+// has already sorted the data, and the launch does nothing.
 __global__ void k_rs_hist(const u32 *__restrict__ keys, u64 n, u32 shift, u32 *__restrict__ hist,
-                          u32 tiles, const u32 *__restrict__ d_n) {
+                          u32 tiles, const u32 *__restrict__ d_n, u32 skip_le) {
+    if (d_n && *d_n <= skip_le) return;
     __shared__ u32 cnt[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) cnt[i] = 0;
     __syncthreads();
@@ -303,7 +310,8 @@ __global__ void k_rs_hist(const u32 *__restrict__ keys, u64 n, u32 shift, u32 *_
 
 __global__ void k_rs_scatter(const u32 *__restrict__ kin, const u32 *__restrict__ vin, u32 *__restrict__ kout,
                              u32 *__restrict__ vout, u64 n, u32 shift, const u32 *__restrict__ offs,
-                             u32 tiles, const u32 *__restrict__ d_n) {
+                             u32 tiles, const u32 *__restrict__ d_n, u32 skip_le) {
+    if (d_n && *d_n <= skip_le) return;
     __shared__ u32 wcnt[RS_WARPS][256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (d_n) n = *d_n;
@@ -410,7 +418,8 @@ __global__ void __launch_bounds__(RSS_WARPS * 32) k_rs_small(u32 *__restrict__ k
     u32 *ka = sm, *va = ka + RSS_CAP, *kb = va + RSS_CAP, *vb = kb + RSS_CAP;
     u32 *wcnt = vb + RSS_CAP;         // [RSS_WARPS][256]
     u32 *dbase = wcnt + RSS_WARPS * 256;  // [257]
-    const u32 n = d_n ? min(*d_n, n_cap) : n_cap;
+    if (d_n && *d_n > n_cap) return;  // more than one block holds: the multi-pass sort takes it
+    const u32 n = d_n ? *d_n : n_cap;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (u32 i = threadIdx.x; i < n; i += blockDim.x) { ka[i] = keys[i]; va[i] = vals[i]; }
     const u32 lt = (1u << lane) - 1u;
@@ -600,15 +609,26 @@ void radix_sort_pairs_dn(Ctx &c, u32 *keys, u32 *vals, const u32 *d_n, u64 n, u3
         LAUNCH(c, k_rs_small, 1, RSS_WARPS * 32, RSS_SMEM, keys, vals, (u32)n, d_n, bits);
         return;
     }
+    // Capacity above one block. With the count on the device both forms are launched: the
+    // one-block sort acts when the count fits it, the passes below when it does not (each kernel
+    // reads the count and returns at once otherwise), and an even number of passes leaves the
+    // data in place either way.
+    u32 skip_le = 0;
+    u32 passes = (bits + 7) / 8;
+    if (d_n) {
+        LAUNCH(c, k_rs_small, 1, RSS_WARPS * 32, RSS_SMEM, keys, vals, (u32)RSS_CAP, d_n, bits);
+        skip_le = RSS_CAP;
+        passes += passes & 1u;
+    }
     size_t m = c.arena.mark();
     const u32 tiles = cdiv(n, RS_TILE);
     u32 *k2 = c.arena.alloc<u32>(n), *v2 = c.arena.alloc<u32>(n);
     u32 *hist = c.arena.alloc<u32>((u64)tiles * 256);
     u32 *ka = keys, *va = vals, *kb = k2, *vb = v2;
-    for (u32 shift = 0; shift < bits; shift += 8) {
-        LAUNCH(c, k_rs_hist, tiles, 256, 0, ka, n, shift, hist, tiles, d_n);
-        scan_excl_u32(c, hist, hist, (u64)tiles * 256);
-        LAUNCH(c, k_rs_scatter, tiles, RS_WARPS * 32, 0, ka, va, kb, vb, n, shift, hist, tiles, d_n);
+    for (u32 pass = 0, shift = 0; pass < passes; ++pass, shift += 8) {
+        LAUNCH(c, k_rs_hist, tiles, 256, 0, ka, n, shift, hist, tiles, d_n, skip_le);
+        scan_impl<u32, u32>(c, hist, hist, (u64)tiles * 256, d_n, skip_le);
+        LAUNCH(c, k_rs_scatter, tiles, RS_WARPS * 32, 0, ka, va, kb, vb, n, shift, hist, tiles, d_n, skip_le);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

@@ -867,12 +867,15 @@ __global__ void k_tier(u32 n, u32 K, const u64 *__restrict__ work, const u64 *__
 }
 
 // ------------------------------------------------------------------ ranking
-// Mover flags, and every node's rank reset (k_set_rank then ranks the movers).
-__global__ void k_move_flags(u32 n, const u32 *__restrict__ target, u32 *__restrict__ flag, u32 *__restrict__ rank) {
+// Mover flags, and every node's rank reset (k_set_rank then ranks the movers) and cascaded gain
+// zeroed.
+__global__ void k_move_flags(u32 n, const u32 *__restrict__ target, u32 *__restrict__ flag, u32 *__restrict__ rank,
+                             unsigned long long *__restrict__ g2) {
     u32 v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) {
         flag[v] = target[v] != NONE ? 1u : 0u;
         rank[v] = NONE;
+        g2[v] = 0;
     }
 }
 __global__ void k_move_keys(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const i64 *__restrict__ gain,
@@ -883,12 +886,13 @@ __global__ void k_move_keys(const u32 *__restrict__ mv, const u32 *__restrict__ 
     hi[i] = (u32)(k >> 32);
     lo[i] = (u32)k;
 }
-__global__ void k_set_rank(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 *__restrict__ rank) {
+// rank[mv[i]] = i; also the size-event count 2M into *twice.
+__global__ void k_set_rank(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 *__restrict__ rank,
+                           u32 *__restrict__ twice) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *twice = 2 * *dM;
     if (i < *dM) rank[mv[i]] = i;
 }
-// small per-round counters derived on the device: [0] M, [1] 2M, [2] inbound events, [3] T
-__global__ void k_twice(const u32 *__restrict__ dM, u32 *__restrict__ out) { *out = 2 * *dM; }
 
 // ------------------------------------------------------------------ cascade
 constexpr u32 CC_WARPS = 4;
@@ -1402,16 +1406,16 @@ __global__ void k_gather_by_dn(const u32 *__restrict__ src, const u32 *__restric
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < *dn) dst[i] = src[idx[i]];
 }
-__global__ void k_clamp_count(u32 *__restrict__ cnt, u64 cap) {
-    if (*cnt > cap) *cnt = (u32)cap;
-}
 // transition keys: (partition, rank) in one word when both fit, else the rank alone (the
-// partition is then a second stable pass)
-__global__ void k_trans_keys(const u32 *__restrict__ dT, u64 nmax, const u32 *__restrict__ tp,
+// partition is then a second stable pass). The count is clamped to the capacity nmax first (an
+// overflow has already set the status word); later kernels read the clamped count.
+__global__ void k_trans_keys(u32 *__restrict__ dT, u64 nmax, const u32 *__restrict__ tp,
                              const u32 *__restrict__ tr, u32 rbits, int combined, u32 *__restrict__ key,
                              u32 *__restrict__ perm) {
     u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= *dT) return;
+    const u64 cnt = *dT < nmax ? *dT : nmax;
+    if (j == 0 && cnt < *dT) atomicMin(dT, (u32)cnt);
+    if (j >= cnt) return;
     key[j] = combined ? ((tp[j] << rbits) | tr[j]) : tr[j];
     perm[j] = (u32)j;
 }
@@ -1892,7 +1896,8 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4;
     // movers in id order, then ranked by (gain desc, id asc)
     u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n), *rank = c.arena.alloc<u32>(n);
-    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag, rank);
+    unsigned long long *g2 = c.arena.alloc<unsigned long long>(n);  // cascaded gains, zeroed here
+    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag, rank, g2);
     compact_indices_dn(c, flag, mv, n, dM);
     const u32 kb = bits_for(lp.gain_bound);
     u32 *khi = c.arena.alloc<u32>(n), *klo = c.arena.alloc<u32>(n);
@@ -1907,10 +1912,9 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     } else {
         radix_sort_pairs_dn(c, klo, mv, dM, n, kb);
     }
-    LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank);
+    LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank, dSE);
     // cascade
-    unsigned long long *g2 = c.arena.alloc<unsigned long long>(n);
-    AXC_CUDA(cudaMemsetAsync(g2, 0, (size_t)n * 8, c.stream));
+
     // inbound-set transitions (INCC): each destination pin of a mover gives at most two
     const bool track = rp.delta < 0x7FFFFFFFu && lp.dst_pins;
     const u64 tcap = track ? 2 * lp.dst_pins : 0;
@@ -1973,7 +1977,6 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     {
         size_t m1 = c.arena.mark();
         const u32 nemax = 2 * n;
-        LAUNCH(c, k_twice, 1, 1, 0, dM, dSE);
         u32 *key = c.arena.alloc<u32>(nemax), *val = c.arena.alloc<u32>(nemax);
         LAUNCH(c, k_size_events, cdiv(nemax, 256), 256, 0, mv, dM, part, target, key, val);
         radix_sort_pairs_dn(c, key, val, dSE, nemax, bits_for(rp.K ? rp.K - 1 : 0));
@@ -1991,7 +1994,6 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         const u64 nt = tcap;
         const u32 rb = bits_for(n ? n - 1 : 0), pb = bits_for(rp.K ? rp.K - 1 : 0);
         const bool combined = rb + pb <= 32;
-        LAUNCH(c, k_clamp_count, 1, 1, 0, dT, nt);  // an overflow already set the status word
         u32 *key = c.arena.alloc<u32>(nt), *perm = c.arena.alloc<u32>(nt);
         LAUNCH(c, k_trans_keys, cdiv(nt, 256), 256, 0, dT, nt, tp, tr, rb, combined ? 1 : 0, key, perm);
         if (combined) {
