@@ -2,10 +2,11 @@
 // continuous batching over a pool of lanes. Each lane is a worker thread with its own stream; a
 // job runs on one lane in a device arena of its estimated size. Jobs start in submission order
 // as lanes and device memory free up, with smaller jobs allowed past one that does not fit yet,
-// so independent jobs overlap on the device.
+// so independent jobs overlap on the device; a job of 1M pins or more runs alone.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -30,6 +31,8 @@ struct Job {
     std::vector<uint32_t> part;
     axc_stats st{};
     size_t est = 0;  // device bytes granted
+    uint64_t pins = 0;
+    bool exclusive = false;  // running alone on the device
     int retries = 0;
     int rc = 0;
     bool done = false;
@@ -60,12 +63,26 @@ struct Executor {
     uint32_t running = 0;
     bool stop = false;
     uint64_t next_id = 1;
+    // Jobs of at least excl_pins pins (0: none) run alone: one such job keeps the GPU busy by
+    // itself, and overlapping it only adds contention; smaller, launch-bound jobs overlap. The
+    // environment variable AXC_SERVE_EXCLUSIVE_PINS overrides the default of 1M pins.
+    uint64_t excl_pins = 1000000;
+    bool excl_running = false;
 
     // The first queued job that fits next to the running ones; with nothing running, the head.
+    // A large job waits until the device drains, and no later job passes it meanwhile.
     Job *pick() {
+        if (excl_running) return nullptr;
         for (auto it = queue.begin(); it != queue.end(); ++it) {
-            if (running == 0 || (*it)->est <= budget - std::min(budget, in_use)) {
-                Job *j = *it;
+            Job *j = *it;
+            if (excl_pins && j->pins >= excl_pins) {
+                if (running) return nullptr;
+                queue.erase(it);
+                j->exclusive = true;
+                excl_running = true;
+                return j;
+            }
+            if (running == 0 || j->est <= budget - std::min(budget, in_use)) {
                 queue.erase(it);
                 return j;
             }
@@ -93,6 +110,10 @@ struct Executor {
                 std::lock_guard<std::mutex> lk(mu);
                 in_use -= j->est;
                 --running;
+                if (j->exclusive) {
+                    j->exclusive = false;
+                    excl_running = false;
+                }
                 if (rc == AXC_ENOMEM && j->retries == 0) {
                     j->retries = 1;
                     j->est *= 2;
@@ -153,6 +174,7 @@ static Executor *executor_for(axc_ctx *ctx, int *rc) {
     size_t budget = cfg != g_config.end() ? cfg->second.second : 0;
     if (budget == 0) budget = device_free_bytes(ctx_device(ctx)) / 2;
     x->budget = budget;
+    if (const char *e = std::getenv("AXC_SERVE_EXCLUSIVE_PINS")) x->excl_pins = std::strtoull(e, nullptr, 10);
     *rc = x->start(ctx_device(ctx));
     if (*rc) return nullptr;
     Executor *p = x.get();
@@ -208,6 +230,7 @@ extern "C" int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p
     j->p = *p;
     j->part.assign(g->n ? g->n : 1, 0);
     j->est = estimate_bytes(g);
+    j->pins = P;
     int rc = AXC_OK;
     Executor *x = executor_for(ctx, &rc);
     if (!x) return rc;
