@@ -3,13 +3,16 @@
 //
 // One round:
 //  1. census: for every hyperedge the partitions among its pins with (pins, destination pins),
-//     in first-occurrence order; partition sizes and distinct-inbound counts.
+//     in first-occurrence order (hashed) or ascending order (partition-indexed, K <= 256);
+//     partition sizes and distinct-inbound counts.
 //  2. gains: every node's best feasible target among the partitions adjacent to it; only moves
-//     with positive gain are proposed.
+//     with positive gain are proposed. With K <= 256 from per-hyperedge partition bitmasks
+//     (O(K/32) per incidence and lane), else from hash tables (O(lambda) per incidence).
 //  3. rank by (gain desc, id asc).
 //  4. cascade: each move's gain recomputed assuming every better-ranked move is applied, by a
 //     sweep over each hyperedge's movers in rank order (O(pins) instead of the reference's
-//     per-move re-read of every incident hyperedge).
+//     per-move re-read of every incident hyperedge), 32 movers at a time per warp with exact
+//     prefix counts.
 //  5. prefix sums of cascaded gains; size-excess and inbound-validity of every prefix from sorted
 //     event streams (sources/refinement.cu:239-491); best prefix by best_move_functor
 //     (headers/data_types.cuh:113-136); apply when valid with non-negative prefix gain.
