@@ -159,6 +159,21 @@ def test_quotient_hypergraph_connectivity_matches_metric():
     assert abs(lam_minus_1 - ev["connectivity_fx"] / 262144.0) < 1e-6
 
 
+def test_context_entry_points_reject_missing_arguments():
+    """Calls that need a context return AXC_EINVAL for a missing one before touching a GPU."""
+    g = ax.gen_circuit(100, 110, 2, 8, 2.5, 0.9, 0.02, 1)
+    part = np.zeros(g.n, np.uint32)
+    L = ax.lib()
+    q = ax.HGraph()
+    pp = part.ctypes.data_as(C.POINTER(C.c_uint32))
+    assert L.axc_quotient_hgraph_device(None, C.byref(g.c()), pp, C.byref(q)) == 1
+    p = ax.params_kway(2, 0.03)
+    st = ax.Stats()
+    assert L.axc_partition(None, C.byref(g.c()), C.byref(p), pp, C.byref(st)) == 1
+    assert L.axc_evaluate(None, C.byref(g.c()), C.byref(p), pp, C.byref(st)) == 1
+    assert L.axc_serve_configure(None, 2, 0) == 1
+
+
 def test_kway_omega_matches_reference_rule():
     # ceil((1 + eps) * n / k) in float (sources/runconfig.cpp:190)
     for n, k, e in ((200000, 2, 0.03), (200000, 64, 0.03), (1000000, 128, 0.03), (4097, 3, 0.1)):
