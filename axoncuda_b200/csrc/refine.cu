@@ -315,8 +315,8 @@ struct GainArgs {
 constexpr u32 GN_DIRECT_K = 256;
 
 // Slots of a node's table: K (rounded up) when indexed by partition id, else from its work bound.
-// Rounds with K <= GN_DIRECT_K take the mask kernels (k_gain_mask_*), so the table kernels below
-// meet that case only through direct calls; their partition-indexed branches serve it.
+// Rounds with K <= GN_DIRECT_K take the mask kernels (k_gain_mask_*); the partition-indexed
+// branches of the table kernels below are kept so that those kernels stay correct for any K.
 __device__ __forceinline__ bool gain_direct(const GainArgs &A) { return A.K <= GN_DIRECT_K; }
 __device__ __forceinline__ u32 gain_cap(const GainArgs &A, u64 work, u32 cap_max) {
     u32 cap = 32;
