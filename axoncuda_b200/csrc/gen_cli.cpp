@@ -4,6 +4,8 @@
 //   axc_gen snn-large <out> <seed>     20 layers x 50,000, fan-out lognormal(256, 0.8) <= 2048, 70% next layer
 //   axc_gen snn <out> <layers> <width> <fanout> <sigma> <cap> <p_next> <seed>
 //   axc_gen circ <out> <n> <e> <smin> <smax> <alpha> <p_local> <local_frac> <seed>
+// Built from the generator and writer sources alone (no libaxc.so, no CUDA), so a process that
+// only needs the input files loads none of the library.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -35,9 +37,9 @@ int main(int argc, char **argv) {
         std::fprintf(stderr, "unknown kind %s\n", kind.c_str());
         return 2;
     }
-    if (rc) { std::fprintf(stderr, "generation failed: %s\n", axc_strerror(rc)); return 1; }
+    if (rc) { std::fprintf(stderr, "generation failed: axc status %d\n", rc); return 1; }
     rc = axc_write_hgraph(out, &g);
-    if (rc) { std::fprintf(stderr, "write failed: %s\n", axc_strerror(rc)); return 1; }
+    if (rc) { std::fprintf(stderr, "write failed: axc status %d\n", rc); return 1; }
     std::printf("%s: %u nodes, %u hyperedges, %llu pins\n", out, g.n, g.e,
                 (unsigned long long)(g.e ? g.hedge_off[g.e] : 0));
     axc_free_hgraph(&g);

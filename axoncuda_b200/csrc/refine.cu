@@ -840,6 +840,264 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 
     }
 }
 
+// ------------------------------------------------------------------ sampled gains (K > AXC_SPARSE_GAIN_K)
+// With more partitions than AXC_SPARSE_GAIN_K a heavy node's adjacent partitions number in the
+// tens of thousands and no per-node table fits on chip. Its gains follow the sampled rule of
+// include/axc.h in two kernels:
+//  - k_gain_sample (one block per node, the sample table in shared memory) finds the sample
+//    prefix, accumulates the sampled connectivity and, when the prefix is the whole node, settles
+//    the node exactly as k_gain_block would; otherwise it writes the node's candidates;
+//  - k_gain_cands (one block per node, no table) sums every incidence's census entries against
+//    those few candidates in registers and picks the best feasible one.
+constexpr u32 GS_K = AXC_SPARSE_GAIN_K;
+constexpr u32 GS_SAMPLE = AXC_SPARSE_GAIN_SAMPLE;
+constexpr u32 GS_C = AXC_SPARSE_GAIN_CANDIDATES;
+constexpr u32 GS_TAB = 2 * GS_SAMPLE;                // sample table slots: at most half full
+constexpr u32 GS_BLOCK = 256;
+constexpr size_t GS_SMEM = (size_t)GS_TAB * 16;      // conn u64, keys u32, inbound u32 per slot
+constexpr u32 GS_DONE = 0xFFFFFFFEu;                 // cand[u*GS_C]: settled by the sample kernel
+constexpr u32 GS_TOMB = 0xFFFFFFFEu;                 // a sample-table key taken out of the selection
+constexpr u32 GS_CAND_BLOCK = 256;
+constexpr u32 GS_CAND_PER_SM = 4;                   // resident blocks of k_gain_cands per SM
+// Nodes outside the sampled kernels (gain tiers 0 and 1) have at most GN_BLOCK_W census entries,
+// so their sample would be the whole node and the exact kernels give the rule's result.
+static_assert(GN_BLOCK_W <= GS_SAMPLE, "tier-1 nodes must fit the sample");
+
+// Census entries of u's incidences j = first, first + stride, ... below jend, flattened across the
+// calling warp's lanes in batches of 32 incidences (the scheme of gain_flat): f(k, w, inbound) is
+// called for each entry k, and every incidence adds its weight to wtot once (per lane).
+template <class F>
+__device__ __forceinline__ void census_flat(const GainArgs &A, u32 u, u32 first, u32 stride, u32 jend, i64 &wtot,
+                                            F &&f) {
+    const u32 lane = threadIdx.x & 31u;
+    const u64 t0 = A.toff[u];
+    const u32 nin_u = A.nin[u];
+    for (u32 jb = first; jb < jend; jb += stride) {
+        const u32 j = jb + lane;
+        const bool has = j < jend;
+        const u32 h = has ? A.touch[t0 + j] : 0;
+        const u32 lm = has ? A.lam[h] : 0;
+        const u32 wh = has ? A.wfx[h] : 0;
+        const u64 ah = has ? A.off[h] : 0;
+        const u32 ib = (has && j < nin_u) ? 1u : 0u;
+        wtot += wh;
+        u32 x = lm;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - lm;
+        const u32 chunk = (jend - jb) < 32 ? (jend - jb) : 32;
+        for (u32 fb = 0; fb < total; fb += 32) {
+            const u32 fi = fb + lane;
+            u32 lo = 0, hi = chunk - 1;
+            for (int it = 0; it < 5; ++it) {
+                const u32 mid = (lo + hi + 1) >> 1;
+                const u32 em = __shfl_sync(0xFFFFFFFFu, excl, mid & 31);
+                if (lo < hi) { if (em <= fi) lo = mid; else hi = mid - 1; }
+            }
+            const u32 eo = __shfl_sync(0xFFFFFFFFu, excl, lo);
+            const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, lo);
+            const u32 wo = __shfl_sync(0xFFFFFFFFu, wh, lo);
+            const u32 io = __shfl_sync(0xFFFFFFFFu, ib, lo);
+            if (fi < total) f(ao + (fi - eo), wo, io);
+        }
+    }
+}
+
+// Block-wide sum of a u64 over GS_BLOCK threads (every thread gets it). `sh` holds one word per warp.
+__device__ __forceinline__ u64 block_sum_u64(u64 v, unsigned long long *sh) {
+    v = warp_sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    u64 t = 0;
+    for (u32 i = 0; i < blockDim.x / 32; ++i) t += sh[i];
+    return t;
+}
+
+// Sampled-connectivity order of the candidate selection: (sconn desc, hash desc, id asc) as one
+// (hi, lo) pair compared as unsigned, the larger first.
+struct SKey {
+    u64 hi, lo;
+};
+__device__ __forceinline__ bool skey_better(const SKey &a, const SKey &b) {
+    return a.hi > b.hi || (a.hi == b.hi && a.lo > b.lo);
+}
+
+__global__ void __launch_bounds__(GS_BLOCK) k_gain_sample(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                          u32 *__restrict__ cand) {
+    const GainArgs A = gain_args_now(A0);
+    extern __shared__ unsigned long long gs_dyn[];
+    unsigned long long *sconn = gs_dyn;      // [GS_TAB]
+    u32 *keys = (u32 *)(gs_dyn + GS_TAB);    // [GS_TAB]
+    u32 *sdc = keys + GS_TAB;                // [GS_TAB]
+    __shared__ unsigned long long wsh[GS_BLOCK / 32];
+    __shared__ unsigned long long s_acc;
+    __shared__ Cand cred[GS_BLOCK / 32];
+    __shared__ SKey kred[GS_BLOCK / 32];
+    __shared__ u32 sred[GS_BLOCK / 32];
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
+        const u32 u = list[idx], p = A.part[u];
+        const u64 t0 = A.toff[u];
+        const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
+        for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sconn[i] = 0; sdc[i] = 0; }
+        // 1. the sample: the longest incidence prefix with at most GS_SAMPLE census entries
+        u32 m = 0;
+        u64 acc = 0;
+        for (u32 base = 0; base < deg; base += GS_BLOCK) {
+            const u32 j = base + threadIdx.x;
+            u64 x = j < deg ? (u64)A.lam[A.touch[t0 + j]] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u64 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if ((int)lane >= o) x += y;
+            }
+            if (lane == 31) wsh[warp] = x;
+            __syncthreads();
+            for (u32 i = 0; i < warp; ++i) x += wsh[i];
+            const bool take = j < deg && acc + x <= GS_SAMPLE;
+            const u32 cnt = (u32)__syncthreads_count(take);
+            if (cnt > 0 && threadIdx.x == cnt - 1) s_acc = acc + x;
+            __syncthreads();
+            m += cnt;
+            if (cnt > 0) acc = s_acc;
+            if (cnt < GS_BLOCK) break;
+        }
+        // 2. sampled connectivity; saving and wtot are exact when the sample is the whole node
+        i64 saving = 0, wtot = 0;
+        census_flat(A, u, 32 * warp, GS_BLOCK, m, wtot, [&](u64 k, u32 w, u32 io) {
+            const u32 q = A.cpart[k];
+            if (q == p) { saving += leave_gain(A.encourage, w, A.ccnt[k]); return; }
+            const u32 slot = hash_find_or_insert(keys, GS_TAB - 1, q);
+            if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
+            atomicAdd(&sconn[slot], (unsigned long long)w);
+            if (io && A.cdcnt[k] > 0) atomicAdd(&sdc[slot], 1u);
+        });
+        __syncthreads();
+        const u64 s = A.nsize[u];
+        if (m == deg) {  // 3a. the whole node: exact, as the table kernels
+            saving = (i64)block_sum_u64((u64)saving, wsh);
+            wtot = (i64)block_sum_u64((u64)wtot, wsh);
+            Cand best{INT64_MIN, 0};
+            for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
+                if (keys[i] == NONE) continue;
+                const Cand c = gain_candidate(A, u, keys[i], sconn[i], sdc[i], saving, wtot);
+                if (cand_better(c, best)) best = c;
+            }
+            best = warp_best(best);
+            if (lane == 0) cred[warp] = best;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                Cand b = cred[0];
+                for (u32 i = 1; i < GS_BLOCK / 32; ++i)
+                    if (cand_better(cred[i], b)) b = cred[i];
+                write_move(A, u, b);
+                cand[(u64)u * GS_C] = GS_DONE;
+            }
+            __syncthreads();
+            continue;
+        }
+        // 3b. rule out what the size limit or the inbound bound excludes
+        const u64 in_sample = m < nin_u ? m : nin_u;
+        for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
+            const u32 q = keys[i];
+            if (q == NONE) continue;
+            if (A.psize[q] + s - s / A.discount > A.omega || A.pinb[q] + in_sample - sdc[i] > A.delta) keys[i] = GS_TOMB;
+        }
+        __syncthreads();
+        // 4. the GS_C best by (sampled connectivity, tie hash, -id), one block-wide maximum each
+        for (u32 r = 0; r < GS_C; ++r) {
+            SKey best{0, 0};
+            u32 bslot = NONE;
+            for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
+                const u32 q = keys[i];
+                if (q >= GS_TOMB) continue;
+                const SKey k{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)};
+                if (bslot == NONE || skey_better(k, best)) { best = k; bslot = i; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                SKey o2{__shfl_xor_sync(0xFFFFFFFFu, best.hi, o), __shfl_xor_sync(0xFFFFFFFFu, best.lo, o)};
+                const u32 os = __shfl_xor_sync(0xFFFFFFFFu, bslot, o);
+                if (os != NONE && (bslot == NONE || skey_better(o2, best))) { best = o2; bslot = os; }
+            }
+            if (lane == 0) { kred[warp] = best; sred[warp] = bslot; }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                SKey b = kred[0];
+                u32 bs = sred[0];
+                for (u32 i = 1; i < GS_BLOCK / 32; ++i)
+                    if (sred[i] != NONE && (bs == NONE || skey_better(kred[i], b))) { b = kred[i]; bs = sred[i]; }
+                cand[(u64)u * GS_C + r] = bs == NONE ? NONE : keys[bs];
+                if (bs != NONE) keys[bs] = GS_TOMB;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// The exact pass of the sampled rule: one block per listed node whose sample was not the whole
+// node; its candidates' connectivity and shared inbound counts over all incidences, then the best
+// feasible candidate (the order of gain_candidate).
+__global__ void __launch_bounds__(GS_CAND_BLOCK, GS_CAND_PER_SM) k_gain_cands(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                              const u32 *__restrict__ cand) {
+    const GainArgs A = gain_args_now(A0);
+    __shared__ unsigned long long wsh[GS_CAND_BLOCK / 32];
+    __shared__ unsigned long long csum[GS_CAND_BLOCK / 32][GS_C];
+    __shared__ u32 dsum[GS_CAND_BLOCK / 32][GS_C];
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
+        const u32 u = list[idx];
+        if (cand[(u64)u * GS_C] == GS_DONE) continue;  // uniform over the block
+        const u32 p = A.part[u];
+        const u32 deg = (u32)(A.toff[u + 1] - A.toff[u]);
+        u32 q[GS_C];
+        unsigned long long cc[GS_C];
+        u32 cd[GS_C];
+#pragma unroll
+        for (u32 i = 0; i < GS_C; ++i) {
+            const u32 v = cand[(u64)u * GS_C + i];
+            q[i] = v == NONE ? GS_TOMB : v;  // never equal to a partition id
+            cc[i] = 0;
+            cd[i] = 0;
+        }
+        i64 saving = 0, wtot = 0;
+        census_flat(A, u, 32 * warp, GS_CAND_BLOCK, deg, wtot, [&](u64 k, u32 w, u32 io) {
+            const u32 x = A.cpart[k];
+            if (x == p) { saving += leave_gain(A.encourage, w, A.ccnt[k]); return; }
+            const u32 dd = (io && A.cdcnt[k] > 0) ? 1u : 0u;
+#pragma unroll
+            for (u32 i = 0; i < GS_C; ++i)
+                if (x == q[i]) { cc[i] += w; cd[i] += dd; }
+        });
+        saving = (i64)block_sum_u64((u64)saving, wsh);
+        wtot = (i64)block_sum_u64((u64)wtot, wsh);
+#pragma unroll
+        for (u32 i = 0; i < GS_C; ++i) {
+            const u64 a = warp_sum((u64)cc[i]);
+            const u32 b = warp_sum(cd[i]);
+            if (lane == 0) { csum[warp][i] = a; dsum[warp][i] = b; }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            Cand best{INT64_MIN, 0};
+            for (u32 i = 0; i < GS_C; ++i) {
+                if (q[i] == GS_TOMB) continue;
+                u64 a = 0;
+                u32 b = 0;
+                for (u32 w2 = 0; w2 < GS_CAND_BLOCK / 32; ++w2) { a += csum[w2][i]; b += dsum[w2][i]; }
+                const Cand c = gain_candidate(A, u, q[i], a, b, saving, wtot);
+                if (cand_better(c, best)) best = c;
+            }
+            write_move(A, u, best);
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_list_degree(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ toff,
                               unsigned long long *__restrict__ out) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1581,6 +1839,7 @@ void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_census_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 2 * CS_BLOCK_CAP * 4));
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
     AXC_CUDA(cudaFuncSetAttribute(k_cascade_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_DYN_MAX));
+    AXC_CUDA(cudaFuncSetAttribute(k_gain_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM));
 }
 
 __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
@@ -1755,7 +2014,15 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
         LAUNCH(c, k_gain_block, lp.ncount[1], GN_BLOCK, cap1 * 16, A, lp.ntier[1], lp.ncount[1], (const u32 *)nullptr,
                cap1, (u32 *)nullptr, (u32 *)nullptr, lp.work, 0u, (u32 *)nullptr, (u32 *)nullptr);
     }
-    if (lp.ncount[2]) {
+    if (lp.ncount[2] && A.K > GS_K) {  // the sampled rule (include/axc.h AXC_SPARSE_GAIN_*)
+        size_t m = c.arena.mark();
+        u32 *cand = c.arena.alloc<u32>((u64)L.n * GS_C);
+        const u32 g1 = std::min<u32>(lp.ncount[2], (u32)c.sms);
+        const u32 g2 = std::min<u32>(lp.ncount[2], (u32)c.sms * GS_CAND_PER_SM);
+        LAUNCH(c, k_gain_sample, g1, GS_BLOCK, GS_SMEM, A, lp.ntier[2], lp.ncount[2], cand);
+        LAUNCH(c, k_gain_cands, g2, GS_CAND_BLOCK, 0, A, lp.ntier[2], lp.ncount[2], (const u32 *)cand);
+        c.arena.release(m);
+    } else if (lp.ncount[2]) {
         size_t m = c.arena.mark();
         const u32 *heavy = lp.ntier[2];
         const u32 *dn = nullptr;

@@ -7,10 +7,14 @@ A step partitions one seeded synthetic hypergraph of the named workload end to e
          flushed between steps (outside the timed step);
   e2e    pins/s through axc_partition with pinned host buffers: the upload of the step's input and
          the download of its partition are inside the timed region.
-`--impl reference` times the reference's own implementation of the path on this box: its GPU
-build compiled from the reference sources (oracle/_ref/hgraph_gpu.exe, the span it reports as
-"Total host execution time"), or the CPU port of the oracle where the reference cannot run the
-mode (k-way needs the external Mt-KaHyPar binary).
+Every partition is also scored by the reference grader (grading/grade.cpp, built from the
+reference sources as oracle/_ref/hgrade.exe) from its partition file; that evaluation, timed, is
+the CPU baseline. The other configurations (--configs) follow as sub-results of the same line.
+`--impl reference` times the reference's own implementation of the path on this box, its GPU
+build compiled from the reference sources (oracle/_ref/hgraph_gpu.exe; for k-way, the same
+sources with the reference's dormant GPU initial partitioner in place of the absent Mt-KaHyPar),
+over the span it reports as "Total host execution time". That arm loads none of this
+repository's libraries: its inputs come from the host-only generator binary axoncuda_b200/axc_gen.
 Multi-GPU (torchrun): one partition job does not shard, so every rank runs a replica; timing is
 the max over ranks.
 """
@@ -32,21 +36,81 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# name: description, axc_gen arguments (kind, seed) for the input file, the reference scripts'
+# flags (hgraphs/run_snns.sh:20 for INCC, hgraphs/run_ispd.sh:20 for k-way) and the grader's
+# constraint flags (grading/grade.cpp -m-prt / -k-prt)
 WORKLOADS = {
-    # name: (description, reference CLI flags)
-    "snn-8x512": ("layered SNN 8x512 fan-out 64 seed 0, INCC omega=128 delta=1024 Kmax=1048576",
-                  ["-m", "128", "1024", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"]),
-    "circuit-200k-k2": ("circuit .hgr 200k nodes 220k nets seed 1, k-way k=2 eps=0.03",
-                        ["-k", "2", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
-    "circuit-200k-k64": ("circuit .hgr 200k nodes 220k nets seed 1, k-way k=64 eps=0.03",
-                         ["-k", "64", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
-    "snn-1m-incc": ("large SNN 20x50k lognormal fan-out seed 2, INCC omega=1024 delta=4096 Kmax=1048576",
-                    ["-m", "1024", "4096", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"]),
-    "snn-1m-k128": ("large SNN 20x50k lognormal fan-out seed 2, k-way k=128 eps=0.03",
-                    ["-k", "128", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"]),
+    "snn-8x512": dict(
+        desc="layered SNN 8x512 fan-out 64 seed 0, INCC omega=128 delta=1024 Kmax=1048576",
+        gen=("snn-layered", "0", ".snn"), kway=False,
+        ref=["-m", "128", "1024", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"],
+        grade=["-m-prt", "128", "1024", "1048576"]),
+    "circuit-200k-k2": dict(
+        desc="circuit .hgr 200k nodes 220k nets seed 1, k-way k=2 eps=0.03",
+        gen=("circuit", "1", ".hgr"), kway=True,
+        ref=["-k", "2", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"],
+        grade=["-k-prt", "2", "0.03"]),
+    "circuit-200k-k64": dict(
+        desc="circuit .hgr 200k nodes 220k nets seed 1, k-way k=64 eps=0.03",
+        gen=("circuit", "1", ".hgr"), kway=True,
+        ref=["-k", "64", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"],
+        grade=["-k-prt", "64", "0.03"]),
+    "snn-1m-incc": dict(
+        desc="large SNN 20x50k lognormal fan-out seed 2, INCC omega=1024 delta=4096 Kmax=1048576",
+        gen=("snn-large", "2", ".snn"), kway=False,
+        ref=["-m", "1024", "4096", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"],
+        grade=["-m-prt", "1024", "4096", "1048576"]),
+    "snn-1m-k128": dict(
+        desc="large SNN 20x50k lognormal fan-out seed 2, k-way k=128 eps=0.03",
+        gen=("snn-large", "2", ".snn"), kway=True,
+        ref=["-k", "128", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"],
+        grade=["-k-prt", "128", "0.03"]),
 }
 DEFAULT_WORKLOAD = "snn-8x512"
+# the other configurations, measured in the same run as per-config sub-results of the line
+DEFAULT_CONFIGS = ["circuit-200k-k2", "circuit-200k-k64", "snn-1m-k128"]
 METRIC = "pins/s end-to-end at equal lambda-1"
+L2_NOTE = "cold between timed steps: a 256 MiB write flushes L2 (the reference arm runs a fresh process per step)"
+GEN = os.path.join(ROOT, "axoncuda_b200", "axc_gen")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def gen_file(name: str, td: str):
+    """Writes the workload's input file with the host-only generator binary (no library loaded in
+    this process) and returns (path, nodes, hyperedges, pins)."""
+    kind, seed, ext = WORKLOADS[name]["gen"]
+    path = os.path.join(td, name + ext)
+    r = subprocess.run([GEN, kind, path, seed], capture_output=True, text=True, check=True)
+    m = re.search(r"(\d+) nodes, (\d+) hyperedges, (\d+) pins", r.stdout)
+    return path, int(m.group(1)), int(m.group(2)), int(m.group(3))
+
+
+def config_of(name: str, nodes: int, hedges: int, pins: int, world: int) -> dict:
+    """The line's config: the same keys and values on both arms."""
+    return {"workload": name, "description": WORKLOADS[name]["desc"], "pins": pins, "nodes": nodes,
+            "hyperedges": hedges, "parallelism": f"replicas x{world}", "l2": L2_NOTE}
+
+
+def grade(path: str, part_path: str, name: str, timeout: float) -> dict:
+    """lambda-1 and validity of a partition file by the reference grader (grading/grade.cpp, built
+    from the reference sources as oracle/_ref/hgrade.exe), with its wall time."""
+    exe = os.path.join(REF_DIR, "hgrade.exe")
+    if not os.path.exists(exe):
+        return {"grader": "unavailable: oracle/_ref/hgrade.exe not built"}
+    t0 = time.perf_counter()
+    try:
+        r = subprocess.run([exe, "-r", path, "-prt", part_path, *WORKLOADS[name]["grade"]], capture_output=True,
+                           text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"grader": f"did not finish within {timeout:.0f} s"}
+    dt = time.perf_counter() - t0
+    out = {"valid": int(r.returncode == 0 and "invalid partitioning" not in r.stderr), "grader_s": dt}
+    for line in r.stdout.splitlines():
+        s = line.strip()
+        for key, nm in (("Connectivity:", "connectivity"), ("Cut-net:", "cutnet"), ("Nodes:", "num_parts")):
+            if s.startswith(key):
+                out[nm] = float(s.split(":", 1)[1].split()[0])
+    return out
 
 
 class Clocks:
@@ -143,7 +207,7 @@ def barrier(world):
         dist.barrier()
 
 
-ROOFLINE_KERNEL = "k_rate_block"  # the kernel with the largest share of device time (profiles/)
+ROOFLINE_KERNEL = "k_rate_block"  # the kernel with the largest share of device time at the default workload
 # algorithmic bytes per launch of the kernels the library's timer has a byte model for
 BYTE_MODELS = {
     "k_rate_block": "4 B per pin visit of the listed nodes (the pin id) + 8 B per candidate slot written",
@@ -152,6 +216,11 @@ BYTE_MODELS = {
     "k_gain_mask_warp": "8 B per incidence entry of the listed nodes + 16 B per listed node",
     "k_gain_mask_block": "8 B per incidence entry of the listed nodes + 16 B per listed node",
 }
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch from one ncu capture of the
+# kernel on the workload, recorded with its capture command in profiles/<kernel>-<workload>.md
+PROFILED_TRAFFIC = {("k_rate_block", "snn-8x512"): 616456}
+STEP_MODEL = ("construction 8P+8(n+E); per rated level 4 B per rating pin visit + 4P_l + 16 n_l C (matching); "
+              "per contraction 8P_l + 12P_(l+1); per refinement round 16P_l + 16n_l (moves not counted)")
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -163,36 +232,39 @@ def hbm_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of the kernel from its committed ncu summary, if there is one."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}-{workload}.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9]+)", line)
-                if m:
-                    return int(m.group(1))
-    except OSError:
-        pass
-    return None
+def step_bytes(st, n0: int, e: int, cnc: int) -> int:
+    """Algorithmic bytes of one whole partition from its per-level sizes (no credit for reuse):
+    level 0 construction, the rating, matching and contraction of every coarsened level, and each
+    refinement round actually run."""
+    L = int(st.levels)
+    P = [int(st.level_pins[l]) for l in range(min(L, 64))]
+    n = [int(st.level_nodes[l]) for l in range(min(L, 64))]
+    total = 8 * P[0] + 8 * (n0 + e) + 4 * int(st.rating_pin_visits)
+    for l in range(len(P)):
+        total += 4 * P[l] + 16 * n[l] * cnc
+        if l + 1 < len(P):
+            total += 8 * P[l] + 12 * P[l + 1]
+        total += int(st.refine_rounds[l]) * (16 * P[l] + 16 * n[l])
+    return total
 
 
-def run_ours(args, world, rank, local):
+def measure_ours(ctx, name: str, steps: int, warmup: int, world: int, td: str, clocks: bool = True,
+                 roofline_kernel: str | None = None, grade_timeout: float = 120.0) -> dict:
+    """One workload on our arm: `value` from device-resident input, `e2e` through the host-buffer
+    call, quality from the library and from the reference grader on the partition file."""
+    import ctypes as C
+
     import torch
 
     import axoncuda_b200 as ax
-    g, p = ax.workload(args.workload)
+    g, p = ax.workload(name)
     P = g.P
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    ctx = ax.Context(local, 0)
-    # ---- device-resident input (value) ----
+    dev = torch.device("cuda", torch.cuda.current_device())
     d_off = torch.from_numpy(g.off.astype(np.uint64).view(np.int64)).to(dev)
     d_pins = torch.from_numpy(g.pins.view(np.int32)).to(dev)
     d_ns = torch.from_numpy(g.nsrc.view(np.int32)).to(dev)
     d_w = torch.from_numpy(g.w).to(dev)
     d_out = torch.empty(max(g.n, 1), dtype=torch.int32, device=dev)
-    import ctypes as C
     dg = ax.HGraph(g.n, g.e, C.cast(d_off.data_ptr(), C.POINTER(C.c_uint64)),
                    C.cast(d_pins.data_ptr(), C.POINTER(C.c_uint32)), C.cast(d_ns.data_ptr(), C.POINTER(C.c_uint32)),
                    C.cast(d_w.data_ptr(), C.POINTER(C.c_float)), None)
@@ -205,18 +277,19 @@ def run_ours(args, world, rank, local):
         if rc:
             raise ax.AxcError(rc, ax.lib().axc_last_error(ctx._h).decode())
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         dev_step()
     torch.cuda.synchronize()
-    total_ms = 0.0
-    launches = 0
-    # the dominant kernel is timed with events on the library's own stream, launch by launch
-    kname = args.roofline_kernel
-    ctx.profile_kernel(kname)
-    ctx.profile_read()
+    total_ms, launches = 0.0, 0
+    if roofline_kernel:
+        ctx.profile_kernel(roofline_kernel)
+        ctx.profile_read()
     k_launches, k_ms, k_bytes = 0, 0.0, 0
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
+    clk = Clocks(torch.cuda.current_device()) if clocks else None
+    if clk:
+        clk.__enter__()
+    try:
+        for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
             barrier(world)
@@ -227,14 +300,19 @@ def run_ours(args, world, rank, local):
             torch.cuda.synchronize()
             total_ms += e0.elapsed_time(e1)
             launches += int(st.kernel_launches)
-            kt = ctx.profile_read()
-            k_launches += kt.launches
-            k_ms += kt.ms_total
-            k_bytes += kt.bytes
-    ctx.profile_kernel(None)
+            if roofline_kernel:
+                kt = ctx.profile_read()
+                k_launches += kt.launches
+                k_ms += kt.ms_total
+                k_bytes += kt.bytes
+    finally:
+        if clk:
+            clk.__exit__(None, None, None)
+    if roofline_kernel:
+        ctx.profile_kernel(None)
     total_ms = barrier_max(world, total_ms)
-    ms_step = total_ms / args.steps
-    value = world * P / (ms_step / 1e3)
+    ms_step = total_ms / steps
+    sbytes = step_bytes(st, g.n, g.e, int(p.cnc))
     # ---- end to end through the host-buffer C-ABI call (pinned buffers) ----
     h_off = torch.from_numpy(g.off.view(np.int64)).pin_memory()
     h_pins = torch.from_numpy(g.pins.view(np.int32)).pin_memory()
@@ -252,10 +330,10 @@ def run_ours(args, world, rank, local):
         if rc:
             raise ax.AxcError(rc, ax.lib().axc_last_error(ctx._h).decode())
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, min(warmup, 3))):
         e2e_step()
     e2e_ms = 0.0
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         barrier(world)
@@ -263,123 +341,182 @@ def run_ours(args, world, rank, local):
         e2e_step()
         e2e_ms += (time.perf_counter() - t0) * 1e3
     e2e_ms = barrier_max(world, e2e_ms)
-    e2e_step_ms = e2e_ms / args.steps
+    e2e_step_ms = e2e_ms / steps
     part = h_out.numpy()[: g.n].view(np.uint32).copy()
     h2d = g.off.nbytes + g.pins.nbytes + g.nsrc.nbytes + g.w.nbytes
-    d2h = 4 * g.n
+    peak, peak_kind = hbm_peak()
     out = {
-        "metric": METRIC, "value": value, "unit": "pins/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload][0], "pins": P,
-                   "nodes": g.n, "hyperedges": g.e, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MiB write) between timed steps"},
+        "value": world * P / (ms_step / 1e3), "ms_per_step": ms_step, "steps": steps, "warmup": warmup,
+        "config": config_of(name, g.n, g.e, P, world),
         "e2e": {"value": world * P / (e2e_step_ms / 1e3), "unit": "pins/s", "ms_per_step": e2e_step_ms,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 * g.n},
         "gpu_launches": launches,
         "quality": {"connectivity": st2.connectivity, "cutnet": st2.cutnet, "num_parts": int(st2.num_parts),
                     "valid": int(st2.valid), "levels": int(st2.levels)},
-        "clocks": clk.summary(),
+        "step_bytes": sbytes, "step_gbs": sbytes / (ms_step / 1e3) / 1e9,
+        "step_frac": sbytes / (ms_step / 1e3) / 1e9 / peak,
+        "peak_device_gb": int(st.device_bytes_peak) / 1e9,
     }
-    peak, peak_kind = hbm_peak()
-    achieved = (k_bytes / (k_ms / 1e3)) / 1e9 if k_ms > 0 else 0.0
-    traffic = profiled_traffic(kname, args.workload)
-    out["roofline"] = {
-        "bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak if peak else None, "peak_source": peak_kind,
-        "traffic": traffic,
-        "bytes_per_launch": k_bytes / k_launches if k_launches else 0,
-        "ms_per_launch": k_ms / k_launches if k_launches else 0,
-        "launches_per_step": k_launches / args.steps,
-        "share_of_step": (k_ms / args.steps) / ms_step if ms_step else None,
-        "model": BYTE_MODELS.get(kname, "none: achieved is 0"),
-    }
-    ctx.close()
-    return out, g, p, part
+    if clk:
+        out["clocks"] = clk.summary()
+    if roofline_kernel:
+        achieved = (k_bytes / (k_ms / 1e3)) / 1e9 if k_ms > 0 else 0.0
+        out["kernel"] = {"achieved": achieved, "k_launches": k_launches, "k_ms": k_ms, "k_bytes": k_bytes,
+                         "peak": peak, "peak_kind": peak_kind}
+    # the reference grader's verdict on this partition (outside every timed region)
+    path, _, _, _ = gen_file(name, td)
+    pf = os.path.join(td, name + ".part")
+    np.savetxt(pf, part, fmt="%d")
+    out["graded"] = grade(path, pf, name, grade_timeout)
+    out["_partfile"] = (path, pf)
+    return out
 
 
-CPU_SAMPLE_PINS = 5_000_000  # above this the CPU baseline times a smaller instance of the generator
+def run_ours(args, world, rank, local):
+    import torch
 
-
-def cpu_sample(name: str, g, p):
-    """The workload itself when the oracle finishes it in seconds, else a smaller instance of the same
-    generator with the same parameters (the large SNN at 20 x 500 neurons), with its description."""
     import axoncuda_b200 as ax
-    if g.P > CPU_SAMPLE_PINS and name.startswith("snn-1m"):
-        gs = ax.gen_snn(20, 500, 256, 0.8, 2048, 0.7, 2)
-        return gs, (f"one full step of the same generator at 20 x 500 neurons ({gs.P} pins; the workload has "
-                    f"{g.P}), same parameters")
-    return g, f"one full step of the workload ({g.P} pins)"
+    torch.cuda.set_device(local)
+    ctx = ax.Context(local, int(args.arena_gb * (1 << 30)))
+    td = tempfile.mkdtemp(prefix="axc_bench_")
+    kname = args.roofline_kernel
+    head = measure_ours(ctx, args.workload, args.steps, args.warmup, world, td, roofline_kernel=kname)
+    peak, peak_kind = hbm_peak()
+    kt = head.pop("kernel")
+    P = head["config"]["pins"]
+    out = {"metric": METRIC, "value": head["value"], "unit": "pins/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
+           "config": head["config"], "e2e": head["e2e"], "gpu_launches": head["gpu_launches"],
+           "quality": dict(head["quality"], grader=head["graded"]), "clocks": head["clocks"]}
+    out["roofline"] = {
+        "bound": "hbm", "kernel": kname, "achieved": kt["achieved"], "peak": peak, "unit": "GB/s",
+        "frac": kt["achieved"] / peak if peak else None, "peak_source": peak_kind,
+        "traffic": PROFILED_TRAFFIC.get((kname, args.workload)),
+        "bytes_per_launch": kt["k_bytes"] / kt["k_launches"] if kt["k_launches"] else 0,
+        "ms_per_launch": kt["k_ms"] / kt["k_launches"] if kt["k_launches"] else 0,
+        "launches_per_step": kt["k_launches"] / args.steps,
+        "share_of_step": (kt["k_ms"] / args.steps) / head["ms_per_step"] if head["ms_per_step"] else None,
+        "model": BYTE_MODELS.get(kname, "none: achieved is 0"),
+        "step_bytes": head["step_bytes"], "step_achieved": head["step_gbs"], "step_frac": head["step_frac"],
+        "step_model": STEP_MODEL,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        path, pf = head["_partfile"]
+        out["cpu_baseline"] = grader_baseline(path, pf, args.workload, P)
+    # the other configurations, fewer steps each (the step count is in each entry)
+    subs = {}
+    for name in ([] if args.configs == "none" else args.configs.split(",")):
+        if name == args.workload:
+            continue
+        large = name.startswith("snn-1m")
+        try:
+            r = measure_ours(ctx, name, 1 if large else 3, 1 if large else 3, world, td, clocks=True,
+                             grade_timeout=300.0 if large else 60.0)
+        except Exception as exc:  # a failing configuration is reported, not fatal to the line
+            subs[name] = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+            continue
+        r.pop("_partfile")
+        subs[name] = {k: r[k] for k in ("value", "ms_per_step", "steps", "warmup", "e2e", "quality", "graded",
+                                       "step_bytes", "step_frac", "peak_device_gb", "clocks", "gpu_launches")}
+        subs[name]["config"] = r["config"]
+    if subs:
+        out["configs"] = subs
+    ctx.close()
+    return out
 
 
-def cpu_port_baseline(g, p, name: str) -> dict:
-    from oracle import oracle as O
-    gs, what = cpu_sample(name, g, p)
-    t0 = time.perf_counter()
-    if p.mode == 0:
-        O.partition(gs.n, gs.off, gs.pins, gs.nsrc, gs.w, 0, omega=p.omega, delta=p.delta, max_parts=p.max_parts,
-                    cnc=p.cnc, rfr=p.rfr, ipm=p.ipm, seed=p.seed)
-    else:
-        O.partition(gs.n, gs.off, gs.pins, gs.nsrc, gs.w, 1, k=p.k, eps=p.eps, cnc=p.cnc, rfr=p.rfr, seed=p.seed)
-    dt = time.perf_counter() - t0
-    return {"value": gs.P / dt, "unit": "pins/s", "cores": 1, "kind": "port",
-            "sample": f"{what} through the oracle's single-threaded C++ restatement of the whole partitioner, "
-                      f"{dt:.2f} s"}
+def grader_baseline(path: str, pf: str, name: str, pins: int) -> dict:
+    """The CPU path of the metric: the reference grader's evaluation (grading/grade.cpp, compiled
+    here as oracle/_ref/hgrade.exe; Mt-KaHyPar is not installable offline) of this run's partition,
+    timed around the process. It is single-threaded."""
+    reps, total, last = 0, 0.0, {}
+    while reps < 50 and total < 15.0:
+        last = grade(path, pf, name, 300.0)
+        if "grader_s" not in last:
+            return {"value": None, "unit": "pins/s", "cores": 1, "kind": "reference",
+                    "sample": f"grade.cpp evaluation: {last.get('grader')}"}
+        total += last["grader_s"]
+        reps += 1
+    return {"value": pins * reps / total, "unit": "pins/s", "cores": 1, "kind": "reference",
+            "host_cores": os.cpu_count(),
+            "sample": f"grade.cpp evaluation (oracle/_ref/hgrade.exe: read, constraint check, lambda-1) of this "
+                      f"run's partition of the full workload ({pins} pins), {reps} runs in {total:.2f} s, "
+                      f"1 thread of {os.cpu_count()} host cores"}
+
+
+def run_reference_one(name: str, steps: int, warmup: int, td: str, timeout: float) -> dict:
+    """The reference GPU build on one workload: its own executable and stdout, this box's B200.
+    INCC runs hgraph_gpu.exe; k-way runs hgraph_gpu_gpuinit.exe, the same sources with the
+    reference's dormant GPU initial partitioner in place of Mt-KaHyPar (absent offline)."""
+    w = WORKLOADS[name]
+    exe = os.path.join(REF_DIR, "hgraph_gpu_gpuinit.exe" if w["kway"] else "hgraph_gpu.exe")
+    path, nodes, hedges, pins = gen_file(name, td)
+    res = {"config": config_of(name, nodes, hedges, pins, 1),
+           "variant": ("reference GPU build with its in-tree GPU initial partitioner (sources/init_part.cu:186-727) "
+                       "in place of Mt-KaHyPar: reference-family, not the Mt-KaHyPar result") if w["kway"]
+           else "reference GPU build (hgraph_gpu.exe, sm_100a, -dlto)"}
+    if not os.path.exists(exe):
+        res["unavailable"] = f"{os.path.relpath(exe, ROOT)} not built"
+        return res
+    times, conn_stdout = [], None
+    pf = os.path.join(td, name + ".ref.part")
+    for i in range(warmup + steps):
+        try:
+            r = subprocess.run([exe, "-r", path, *w["ref"], "-p", pf], capture_output=True, text=True, cwd=td,
+                               timeout=timeout)
+        except subprocess.TimeoutExpired:
+            res["unavailable"] = f"reference did not finish one partition within {timeout:.0f} s"
+            return res
+        if r.returncode != 0:
+            tail = " ".join((r.stderr.strip() or r.stdout.strip()).split())[-240:]
+            res["unavailable"] = f"reference exited {r.returncode}: {tail}"
+            return res
+        m = re.search(r"Total host execution time: ([0-9.]+) ms", r.stdout)
+        if m is None:
+            res["unavailable"] = "reference printed no 'Total host execution time'"
+            return res
+        if i >= warmup:
+            times.append(float(m.group(1)))
+        mc = re.search(r"Connectivity:\s+([0-9.eE+]+)", r.stdout)
+        conn_stdout = float(mc.group(1)) if mc else None
+    ms = sum(times) / len(times)
+    res.update({"value": pins / (ms / 1e3), "ms_per_step": ms, "steps": steps, "warmup": warmup,
+                "graded": grade(path, pf, name, 600.0), "stdout_connectivity": conn_stdout})
+    return res
 
 
 def run_reference(args):
-    """The reference's own implementation of the path, timed on this box."""
-    import axoncuda_b200 as ax
-    g, p = ax.workload(args.workload)
-    exe = os.path.join(ROOT, "oracle", "_ref", "hgraph_gpu.exe")
-    flags = WORKLOADS[args.workload][1]
-    kway = p.mode == ax.MODE_KWAY
+    """The reference's own implementation of the path, timed on this box. This process loads none
+    of the repository's libraries: inputs come from the host-only generator binary, the reference
+    runs as its own executables, and its partitions are scored by its own grader."""
+    td = tempfile.mkdtemp(prefix="axc_ref_")
     line = {"metric": METRIC, "unit": "pins/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][0], "pins": g.P}}
-    if not kway and os.path.exists(exe):
-        with tempfile.TemporaryDirectory() as td:
-            ext = ".hgr" if "circuit" in args.workload else ".snn"
-            path = os.path.join(td, "in" + ext)
-            ax.write(path, g)
-            times = []
-            conn = None
-            for i in range(args.warmup + args.steps):
-                pf = os.path.join(td, "out.part")
-                try:
-                    r = subprocess.run([exe, "-r", path, *flags, "-p", pf], capture_output=True, text=True, cwd=td,
-                                       timeout=args.ref_timeout)
-                except subprocess.TimeoutExpired:
-                    line["unavailable"] = f"reference did not finish one partition within {args.ref_timeout:.0f} s"
-                    return line
-                if r.returncode != 0:
-                    tail = (r.stderr.strip() or r.stdout.strip())[-200:]
-                    line["unavailable"] = f"reference exited {r.returncode}: {tail}"
-                    return line
-                m = re.search(r"Total host execution time: ([0-9.]+) ms", r.stdout)
-                if m is None:
-                    line["unavailable"] = "reference printed no 'Total host execution time'"
-                    return line
-                if i >= args.warmup:
-                    times.append(float(m.group(1)))
-                mc = re.search(r"Connectivity:\s+([0-9.]+)", r.stdout)
-                conn = float(mc.group(1)) if mc else None
-            ms = sum(times) / len(times)
-            v = g.P / (ms / 1e3)
-            line.update({"value": v, "ms_per_step": ms,
-                         "cpu_baseline": {"value": v, "unit": "pins/s", "cores": 0, "kind": "reference",
-                                          "sample": "full workload through the reference GPU build "
-                                                    "(hgraph_gpu.exe, sm_100a), its 'Total host execution time'"},
-                         "e2e": {"value": v, "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                         "quality": {"connectivity": conn}})
-            return line
-    # k-way: the reference needs the external Mt-KaHyPar binary (sources/init_part.cu:891-906), which
-    # is not installable offline; time the oracle's CPU port instead.
-    cb = cpu_port_baseline(g, p, args.workload)
-    line.update({"value": cb["value"], "ms_per_step": g.P / cb["value"] * 1e3, "cpu_baseline": cb,
-                 "e2e": {"value": cb["value"], "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                 "note": "reference k-way needs mtkahypar (absent); CPU port of the oracle timed instead"})
+            "data": "synthetic (seeded generator)", "impl": "reference"}
+    with Clocks(0) as clk:
+        head = run_reference_one(args.workload, args.steps, args.warmup, td, args.ref_timeout)
+    line["config"] = head.pop("config")
+    if "unavailable" in head:
+        line["unavailable"] = head["unavailable"]
+        return line
+    v = head["value"]
+    line.update({"value": v, "ms_per_step": head["ms_per_step"], "variant": head["variant"],
+                 "cpu_baseline": {"value": v, "unit": "pins/s", "cores": 1, "kind": "reference",
+                                  "sample": f"the full workload through {head['variant']}: its 'Total host execution "
+                                            f"time' (upload to partition download), one host thread driving one B200"},
+                 "e2e": {"value": v, "unit": "pins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "quality": {"grader": head["graded"], "stdout_connectivity": head["stdout_connectivity"]},
+                 "clocks": clk.summary()})
+    subs = {}
+    for name in ([] if args.configs == "none" else args.configs.split(",")):
+        if name == args.workload:
+            continue
+        large = name.startswith("snn-1m")
+        r = run_reference_one(name, 1 if large else 2, 0 if large else 1, td, args.ref_timeout)
+        subs[name] = r
+    if subs:
+        line["configs"] = subs
     return line
 
 
@@ -545,6 +682,10 @@ def main():
     ap.add_argument("--serve-max-pins", type=float, default=2e7)
     ap.add_argument("--serve-load", type=float, default=2.0)
     ap.add_argument("--seq-arena-gb", type=float, default=24.0)
+    ap.add_argument("--arena-gb", type=float, default=0.0,
+                    help="device arena of the partition context in GiB (0: the library default, 60%% of free memory)")
+    ap.add_argument("--configs", default=",".join(DEFAULT_CONFIGS),
+                    help="comma-separated other workloads measured as sub-results of the line, or 'none'")
     args = ap.parse_args()
     if args.mode == "batch":
         out = run_batch(args)
@@ -563,10 +704,8 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return
     world, rank, local = dist_setup(args)
-    out, g, p, part = run_ours(args, world, rank, local)
+    out = run_ours(args, world, rank, local)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_port_baseline(g, p, args.workload)
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -83,6 +83,18 @@ typedef struct {
  * everywhere else). The reference rates through every hyperedge (kernels/coarsening.cu:76-202);
  * its pair visits grow as |e|^2, which at 3e8 pins is what exhausts its neighbour lists. */
 #define AXC_RATE_MAX_LEN 128u
+/* Refinement with more than AXC_SPARSE_GAIN_K partitions bounds each node's gain work. A node's
+ * candidate targets come from a sample: the longest prefix of its incidences (inbound hyperedges
+ * first, each part ascending) whose hyperedges hold at most AXC_SPARSE_GAIN_SAMPLE (partition,
+ * hyperedge) census entries in all. When that prefix is the whole node the gains are the exact
+ * ones over every adjacent partition. Otherwise the AXC_SPARSE_GAIN_CANDIDATES partitions with the
+ * largest sampled connectivity that are not already ruled out by the size limit or by an upper
+ * bound of their shared inbound hyperedges are evaluated exactly, and the best feasible one is the
+ * node's target. The reference's dense gain table needs E x K words, which at K near 1e5 does not
+ * fit; its sparse path bounds the work differently (sources/refinement.cu:587-1378). */
+#define AXC_SPARSE_GAIN_K 4096u
+#define AXC_SPARSE_GAIN_SAMPLE 4096u
+#define AXC_SPARSE_GAIN_CANDIDATES 8u
 
 typedef struct {
     uint32_t num_parts;        /* K' after zero-basing */

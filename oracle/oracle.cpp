@@ -20,6 +20,7 @@
 #include <fstream>
 #include <numeric>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -119,7 +120,7 @@ T touching(const G &g) {
 // (their pair visits grow as |e|^2 while each pair gains only floor(w/|e|)); leaving them out of
 // the shared-inbound count only makes the delta filter stricter.
 void rating(const G &g, const std::vector<u32> &wfx, const T &t, const u32 *nsize, u32 omega,
-            u32 delta, u32 cnc, u32 *pairs, u32 *scores) {
+            u32 delta, u32 cnc, u32 *pairs, u32 *scores, u64 max_len = RATE_MAX_LEN) {
     std::vector<u32> sc(g.n, 0), cm(g.n, 0), mark(g.n, NONE);
     std::vector<u32> touched;
     std::vector<std::pair<u32, u32>> cand;
@@ -130,7 +131,7 @@ void rating(const G &g, const std::vector<u32> &wfx, const T &t, const u32 *nsiz
             const u32 h = t.touch[j];
             const bool inb = (j - t0) < t.nin[u];
             const u64 a = g.off[h], b = g.off[h + 1];
-            if (b - a > RATE_MAX_LEN) continue;
+            if (b - a > max_len) continue;
             const u32 c = wfx[h] / (u32)(b - a);
             for (u64 k = a; k < b; ++k) {
                 const u32 v = g.pins[k];
@@ -330,6 +331,12 @@ inline i64 leave_gain(bool encourage, u32 w, u32 c) {
 // adjacent to it (loss(q) = sum of w over incident hyperedges without a pin in q), feasible when
 // size(q) + s - floor(s/discount) <= omega and (this build) size_in(q) + new inbound <= delta;
 // ties go to the larger mix32(q + round + seed), then the smaller id. Only positive gains move.
+// With more than AXC_SPARSE_GAIN_K partitions, a node whose incidences hold more census entries
+// than AXC_SPARSE_GAIN_SAMPLE takes the sampled rule of sampled_target (include/axc.h).
+bool sampled_target(const RefineCtx &rc, const std::vector<u32> &part, const Census &cs,
+                    const std::vector<u64> &psize, const std::vector<u64> &pinb, u32 discount, u32 round,
+                    u32 u, u32 *target, i64 *gain);
+
 void gains(const RefineCtx &rc, const std::vector<u32> &part, const Census &cs,
            const std::vector<u64> &psize, const std::vector<u64> &pinb, u32 discount, u32 round,
            u32 *target, i64 *gain) {
@@ -338,6 +345,8 @@ void gains(const RefineCtx &rc, const std::vector<u32> &part, const Census &cs,
     std::vector<i64> conn(rc.K, 0);
     std::vector<u32> dconn(rc.K, 0), mark(rc.K, NONE), touched;
     for (u32 u = 0; u < g.n; ++u) {
+        if (rc.K > AXC_SPARSE_GAIN_K && sampled_target(rc, part, cs, psize, pinb, discount, round, u, target, gain))
+            continue;
         const u32 p = part[u];
         const u64 s = rc.nsize[u];
         i64 saving = 0, wtot = 0;
@@ -372,6 +381,99 @@ void gains(const RefineCtx &rc, const std::vector<u32> &part, const Census &cs,
         if (best != NONE && bg > 0) { target[u] = best; gain[u] = bg; }
         else { target[u] = NONE; gain[u] = 0; }
     }
+}
+
+// The sampled rule for node u (include/axc.h AXC_SPARSE_GAIN_*). Returns false when u's sample
+// is all of its incidences (the exact rule of gains() then applies, with the same result);
+// otherwise writes u's target and gain.
+//  1. The sample: the longest prefix j < m of u's incidences (touching order: inbound ascending,
+//     then outbound ascending) whose census entries number at most AXC_SPARSE_GAIN_SAMPLE.
+//  2. Sampled connectivity sconn[q] = sum of w over the sample's hyperedges holding q (q != p),
+//     sdc[q] = the sample's inbound hyperedges with destination pins in q.
+//  3. q is ruled out when size(q) + s - floor(s/discount) > omega, or when even the inbound
+//     hyperedges outside the sample all shared with q could not make room:
+//     pinb[q] + min(m, nin_u) - sdc[q] > delta.
+//  4. The first AXC_SPARSE_GAIN_CANDIDATES of the others by (sconn desc, mix32(q + round + seed)
+//     desc, q asc) are evaluated exactly over all incidences, as gains() would; the best feasible
+//     one by (gain desc, hash desc, q asc) is the target when its gain is positive.
+bool sampled_target(const RefineCtx &rc, const std::vector<u32> &part, const Census &cs,
+                    const std::vector<u64> &psize, const std::vector<u64> &pinb, u32 discount, u32 round,
+                    u32 u, u32 *target, i64 *gain) {
+    const T &t = *rc.t;
+    const u64 t0 = t.toff[u], deg = t.toff[u + 1] - t0;
+    const u32 nin = t.nin[u], p = part[u];
+    u64 m = 0, acc = 0;
+    while (m < deg) {
+        const u32 h = t.touch[t0 + m];
+        const u64 lam = cs.beg[h + 1] - cs.beg[h];
+        if (acc + lam > AXC_SPARSE_GAIN_SAMPLE) break;
+        acc += lam;
+        ++m;
+    }
+    if (m == deg) return false;
+    struct Acc { u64 conn = 0; u32 dc = 0; };
+    std::unordered_map<u32, Acc> tab;  // at most AXC_SPARSE_GAIN_SAMPLE entries
+    auto find = [&](u32 q) -> Acc & { return tab[q]; };
+    for (u64 j = 0; j < m; ++j) {
+        const u32 h = t.touch[t0 + j];
+        const u32 w = (*rc.wfx)[h];
+        for (u64 k = cs.beg[h]; k < cs.beg[h + 1]; ++k) {
+            const u32 q = cs.part[k];
+            if (q == p) continue;
+            Acc &a = find(q);
+            a.conn += w;
+            if (j < nin && cs.dcnt[k] > 0) a.dc++;
+        }
+    }
+    const u64 s = rc.nsize[u];
+    const u64 in_sample = std::min<u64>(m, nin);
+    struct Key { u64 conn; u32 hash; u32 q; };
+    std::vector<Key> keys;
+    for (auto &x : tab) {
+        const u32 q = x.first;
+        if (psize[q] + s - s / discount > rc.omega) continue;
+        if (pinb[q] + in_sample - x.second.dc > rc.delta) continue;
+        keys.push_back({x.second.conn, mix32(q + round + (u32)rc.seed), q});
+    }
+    std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+        if (a.conn != b.conn) return a.conn > b.conn;
+        if (a.hash != b.hash) return a.hash > b.hash;
+        return a.q < b.q;
+    });
+    if (keys.size() > AXC_SPARSE_GAIN_CANDIDATES) keys.resize(AXC_SPARSE_GAIN_CANDIDATES);
+    const size_t nc = keys.size();
+    std::vector<i64> conn(nc, 0);
+    std::vector<u32> dconn(nc, 0);
+    i64 saving = 0, wtot = 0;
+    for (u64 j = 0; j < deg; ++j) {
+        const u32 h = t.touch[t0 + j];
+        const u32 w = (*rc.wfx)[h];
+        wtot += w;
+        for (u64 k = cs.beg[h]; k < cs.beg[h + 1]; ++k) {
+            const u32 q = cs.part[k];
+            if (q == p) { saving += leave_gain(rc.encourage, w, cs.cnt[k]); continue; }
+            for (size_t i = 0; i < nc; ++i)
+                if (keys[i].q == q) {
+                    conn[i] += w;
+                    if (j < nin && cs.dcnt[k] > 0) dconn[i]++;
+                }
+        }
+    }
+    u32 best = NONE, bh = 0;
+    i64 bg = 0;
+    for (size_t i = 0; i < nc; ++i) {
+        const u32 q = keys[i].q;
+        if (psize[q] + s - s / discount > rc.omega) continue;
+        if (pinb[q] + (u64)(nin - dconn[i]) > rc.delta) continue;
+        const i64 gq = saving - (wtot - conn[i]);
+        const u32 hq = keys[i].hash;
+        if (best == NONE || gq > bg || (gq == bg && (hq > bh || (hq == bh && q < best)))) {
+            best = q; bg = gq; bh = hq;
+        }
+    }
+    if (best != NONE && bg > 0) { target[u] = best; gain[u] = bg; }
+    else { target[u] = NONE; gain[u] = 0; }
+    return true;
 }
 
 std::vector<u64> part_sizes(const std::vector<u32> &part, const u32 *nsize, u32 K) {
@@ -712,13 +814,22 @@ void or_rating(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins
                const uint32_t *nsrc, const uint32_t *wfx, const uint64_t *toff,
                const uint32_t *touch, const uint32_t *inbound, const uint32_t *node_size,
                uint32_t omega, uint32_t delta, uint32_t cnc, uint32_t *pairs, uint32_t *scores) {
+    or_rating_len(n, e, off, pins, nsrc, wfx, toff, touch, inbound, node_size, omega, delta, cnc, RATE_MAX_LEN,
+                  pairs, scores);
+}
+
+void or_rating_len(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
+                   const uint32_t *nsrc, const uint32_t *wfx, const uint64_t *toff,
+                   const uint32_t *touch, const uint32_t *inbound, const uint32_t *node_size,
+                   uint32_t omega, uint32_t delta, uint32_t cnc, uint64_t max_len, uint32_t *pairs,
+                   uint32_t *scores) {
     G g = mkG(n, e, off, pins, nsrc);
     T t;
     t.toff.assign(toff, toff + n + 1);
     t.touch.assign(touch, touch + toff[n]);
     t.nin.assign(inbound, inbound + n);
     std::vector<u32> w(wfx, wfx + e);
-    rating(g, w, t, node_size, omega, delta, cnc, pairs, scores);
+    rating(g, w, t, node_size, omega, delta, cnc, pairs, scores, max_len);
 }
 
 uint32_t or_matching(uint32_t n, uint32_t cnc, const uint32_t *pairs, const uint32_t *scores,

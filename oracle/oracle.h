@@ -39,6 +39,14 @@ void or_rating(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins
                const uint32_t *nsrc, const uint32_t *wfx, const uint64_t *toff,
                const uint32_t *touch, const uint32_t *inbound, const uint32_t *node_size,
                uint32_t omega, uint32_t delta, uint32_t cnc, uint32_t *pairs, uint32_t *scores);
+/* The same with the hyperedge length limit given: hyperedges of more than max_len pins take no
+ * part (or_rating uses AXC_RATE_MAX_LEN; UINT64_MAX rates through every hyperedge, as the
+ * reference does). */
+void or_rating_len(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
+                   const uint32_t *nsrc, const uint32_t *wfx, const uint64_t *toff,
+                   const uint32_t *touch, const uint32_t *inbound, const uint32_t *node_size,
+                   uint32_t omega, uint32_t delta, uint32_t cnc, uint64_t max_len, uint32_t *pairs,
+                   uint32_t *scores);
 
 /* Matching + orphan pairing + relabel (this build's deterministic propose/accept matching;
  * orphans as sources/chaining.cu:260-329). Returns the number of groups. */

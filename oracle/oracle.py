@@ -88,14 +88,20 @@ def touching(n, off, pins, nsrc):
     return toff, touch[: len(pins)], nin[:n]
 
 
-def rating(n, off, pins, nsrc, wfx_, node_size, omega, delta, cnc):
+RATE_MAX_LEN = 128  # include/axc.h AXC_RATE_MAX_LEN
+NO_LEN_LIMIT = (1 << 64) - 1
+
+
+def rating(n, off, pins, nsrc, wfx_, node_size, omega, delta, cnc, max_len=RATE_MAX_LEN):
+    """Top-cnc candidates per node; hyperedges longer than max_len pins take no part (NO_LEN_LIMIT
+    rates through all of them, as the reference does)."""
     off, pins, nsrc, wfx_, ns = _u64(off), _u32(pins), _u32(nsrc), _u32(wfx_), _u32(node_size)
     toff, touch, nin = touching(n, off, pins, nsrc)
     pairs = np.zeros(max(n * cnc, 1), np.uint32); scores = np.zeros(max(n * cnc, 1), np.uint32)
-    lib().or_rating(C.c_uint32(n), C.c_uint32(len(nsrc)), _p(off, C.c_uint64), _p(pins, C.c_uint32),
-                    _p(nsrc, C.c_uint32), _p(wfx_, C.c_uint32), _p(toff, C.c_uint64), _p(touch, C.c_uint32),
-                    _p(nin, C.c_uint32), _p(ns, C.c_uint32), C.c_uint32(omega), C.c_uint32(delta),
-                    C.c_uint32(cnc), _p(pairs, C.c_uint32), _p(scores, C.c_uint32))
+    lib().or_rating_len(C.c_uint32(n), C.c_uint32(len(nsrc)), _p(off, C.c_uint64), _p(pins, C.c_uint32),
+                        _p(nsrc, C.c_uint32), _p(wfx_, C.c_uint32), _p(toff, C.c_uint64), _p(touch, C.c_uint32),
+                        _p(nin, C.c_uint32), _p(ns, C.c_uint32), C.c_uint32(omega), C.c_uint32(delta),
+                        C.c_uint32(cnc), C.c_uint64(max_len), _p(pairs, C.c_uint32), _p(scores, C.c_uint32))
     return pairs[: n * cnc], scores[: n * cnc]
 
 

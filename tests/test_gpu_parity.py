@@ -170,18 +170,62 @@ def test_cascade_kernels_match_oracle(ctx, monkeypatch, i, block_movers):
         assert st.num_parts > 256
 
 
-# Nodes whose gain-table bound passes 4096 slots (here K = 5000 partitions of two neurons and about
-# 80 inbound hyperedges of about 80 pins) first try a shared-memory table and fall back to a
-# global one when they reach too many distinct partitions. AXC_GAIN_TRY_LIMIT=16 makes nearly
-# every such node fall back.
+# Nodes whose gain-table bound passes 4096 slots (here about 2000 partitions of two neurons and
+# about 80 inbound hyperedges of about 80 pins) first try a shared-memory table and fall back to a
+# global one when they reach too many distinct partitions. With at most 4096 partitions the first
+# try always fits; AXC_GAIN_TRY_LIMIT=16 makes nearly every such node fall back.
 @pytest.mark.parametrize("try_limit", [None, "16"])
 def test_heavy_gain_tier_matches_oracle(ctx, monkeypatch, try_limit):
-    g = ax.gen_snn(4, 2500, 80, 0.7, 300, 0.7, 31)
+    g = ax.gen_snn(4, 1000, 80, 0.7, 300, 0.7, 31)
     p = ax.params_incc(2, 4096, 1048576, cnc=4, rfr=4)
     if try_limit is None:
         monkeypatch.delenv("AXC_GAIN_TRY_LIMIT", raising=False)
     else:
         monkeypatch.setenv("AXC_GAIN_TRY_LIMIT", try_limit)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1 and 256 < st.num_parts <= 4096
+
+
+def census_entries_per_node(g, part):
+    """Sum over each node's incident hyperedges of their distinct partitions (the sample measure of
+    the sampled gain rule)."""
+    off = g.off.astype(np.int64)
+    lens = off[1:] - off[:-1]
+    hid = np.repeat(np.arange(g.e), lens)
+    pairs = np.unique(np.stack([hid, part[g.pins].astype(np.int64)], 1), axis=0)
+    lam = np.bincount(pairs[:, 0], minlength=g.e)
+    return np.bincount(g.pins.astype(np.int64), weights=lam[hid], minlength=g.n)
+
+
+# More than AXC_SPARSE_GAIN_K = 4096 partitions: nodes whose incidences hold more than 4096 census
+# entries take the sampled rule (candidates from an incidence prefix, exact evaluation of the best
+# 8); the others the exact gains. Both against the oracle's restatement of the rule.
+SAMPLED_CASES = [(6000, 1 << 20, 1 << 20, 1, 1), (6000, 40, 150, 1, 2), (9000, 3, 0x7FFFFFFF, 0, 1),
+                 (5000, 1 << 20, 120, 1, 0xFFFFFFFF)]
+
+
+@pytest.mark.parametrize("K,omega,delta,enc,disc", SAMPLED_CASES)
+def test_sampled_gains_match_oracle(ctx, K, omega, delta, enc, disc):
+    g = dedup(ax.gen_snn(4, 3000, 90, 0.5, 400, 0.7, 41))
+    rng = np.random.default_rng(K + disc)
+    part = rng.integers(0, K, g.n).astype(np.uint32)
+    ns = rng.integers(1, 3, g.n).astype(np.uint32)
+    ent = census_entries_per_node(g, part)
+    assert (ent > 4096).sum() > 100 and (ent <= 4096).sum() > 100  # both paths are exercised
+    tgt, gain = ctx.stage_gains(g, part, K, ns, omega, delta, enc, disc)
+    o_tgt, o_gain = O.gains(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, part, K, omega, delta, enc, disc)
+    np.testing.assert_array_equal(tgt, o_tgt)
+    np.testing.assert_array_equal(gain, o_gain)
+    assert (tgt[ent > 4096] != NONE).any()
+
+
+def test_partition_with_sampled_gains_matches_oracle(ctx):
+    """An INCC run whose inbound limit stops coarsening early, so every level refines with more
+    than 4096 partitions and heavy nodes take the sampled rule; equal to the oracle's partition."""
+    g = ax.gen_snn(10, 1000, 80, 0.0, 0, 1.0, 43)
+    p = ax.params_incc(1024, 100, 1048576, cnc=4, rfr=8)
     part, st = ctx.partition(g, p)
     o_part, o_K, _, _ = oracle_partition(g, p)
     np.testing.assert_array_equal(part, o_part)

@@ -118,3 +118,93 @@ def test_oracle_partitioner_valid_and_deterministic(name):
     om = int(np.ceil(np.float32(1.05) * np.float32(n) / np.float32(4)))
     ev = O.evaluate(*args, q1, om, 0x7FFFFFFF, 4)
     assert ev["valid"] == 1
+
+
+# ---- the reference's own coarsening stages (oracle/refstages.cu run on a GPU; fixtures made by
+# tests/golden/make_refstages.py) --------------------------------------------------------------
+REFSTAGE = sorted(f[: -len(".refstage.npz")] for f in os.listdir(GOLDEN) if f.endswith(".refstage.npz"))
+
+
+def refstage(case):
+    name = case.rsplit(".", 1)[0]
+    return name, np.load(os.path.join(GOLDEN, case + ".refstage.npz"))
+
+
+def test_refstage_fixtures_present():
+    """Every input of make_refstages.py has its fixture (loose and tight limits for the synthetic ones)."""
+    assert len(REFSTAGE) >= 9, REFSTAGE
+
+
+@pytest.mark.parametrize("case", REFSTAGE)
+def test_rating_matches_reference_stage(case):
+    """The oracle's rating equals the reference's candidatesProposal (sources/coarsening.cu:17-68,
+    kernels/coarsening.cu:10-213) pair for pair and score for score: same neighbours, same size
+    and inbound filters, same symmetric noise, same top-cnc order. The reference rates through
+    every hyperedge, so the oracle runs without its length limit here."""
+    name, s = refstage(case)
+    r = load(name)
+    n, cnc = int(s["n"]), int(s["cnc"])
+    assert n == int(r["ded_n"]) and int(s["P"]) == len(r["ded_pins"])
+    pairs, scores = O.rating(n, r["ded_off"], r["ded_pins"], r["ded_nsrc"], O.wfx(r["ded_w"]),
+                             np.ones(n, np.uint32), int(s["omega"]), int(s["delta"]), cnc, max_len=O.NO_LEN_LIMIT)
+    np.testing.assert_array_equal(pairs, s["pairs"])
+    ok = s["pairs"] != O.NONE  # the reference leaves the score of an empty slot unwritten
+    np.testing.assert_array_equal(scores[ok], s["scores"][ok])
+
+
+@pytest.mark.parametrize("case", REFSTAGE)
+def test_rating_length_limit_is_inert_below_128(case):
+    """On inputs whose hyperedges all have at most 128 pins, the length limit changes nothing."""
+    name, s = refstage(case)
+    r = load(name)
+    n, cnc = int(s["n"]), int(s["cnc"])
+    off = r["ded_off"].astype(np.int64)
+    if len(off) > 1 and int((off[1:] - off[:-1]).max()) > O.RATE_MAX_LEN:
+        pytest.skip("input has hyperedges above the rating length limit")
+    args = (n, r["ded_off"], r["ded_pins"], r["ded_nsrc"], O.wfx(r["ded_w"]), np.ones(n, np.uint32),
+            int(s["omega"]), int(s["delta"]), cnc)
+    a, _ = O.rating(*args)
+    b, _ = O.rating(*args, max_len=O.NO_LEN_LIMIT)
+    np.testing.assert_array_equal(a, b)
+
+
+def _hedge_sets(off, pins, nsrc):
+    out = []
+    for h in range(len(nsrc)):
+        seg = pins[int(off[h]): int(off[h + 1])]
+        k = int(nsrc[h])
+        out.append((tuple(sorted(seg[:k].tolist())), tuple(sorted(seg[k:].tolist()))))
+    return out
+
+
+@pytest.mark.parametrize("case", REFSTAGE)
+def test_contract_matches_reference_stage(case):
+    """The oracle's contraction of the reference's own grouping equals the reference's
+    coarsenHedges (sources/construction.cu:563-676): the same hyperedge offsets and source counts,
+    and per hyperedge the same source set and destination set (a group that is also a destination
+    leaves the sources; size-1 hyperedges stay). The reference lists destinations descending,
+    the oracle ascending, so the segments are compared as sets."""
+    name, s = refstage(case)
+    r = load(name)
+    off, pins, nsrc = O.contract(r["ded_off"], r["ded_pins"], r["ded_nsrc"], s["groups"])
+    np.testing.assert_array_equal(off, s["coff"])
+    np.testing.assert_array_equal(nsrc, s["cnsrc"])
+    assert _hedge_sets(off, pins, nsrc) == _hedge_sets(s["coff"], s["cpins"], s["cnsrc"])
+
+
+@pytest.mark.parametrize("case", REFSTAGE)
+def test_coarse_incidence_matches_reference_stage(case):
+    """Incidence sets of the contracted graph equal the reference's coarsenTouching
+    (sources/construction.cu:678-789): per coarse node the same inbound hyperedges and the same
+    outbound ones (an edge in both stays inbound only), both in ascending order."""
+    name, s = refstage(case)
+    r = load(name)
+    off, pins, nsrc = O.contract(r["ded_off"], r["ded_pins"], r["ded_nsrc"], s["groups"])
+    toff, touch, nin = O.touching(int(s["ngroups"]), off, pins, nsrc)
+    np.testing.assert_array_equal(nin, s["cinb"])
+    np.testing.assert_array_equal(toff, s["ctoff"])
+    for v in range(int(s["ngroups"])):
+        a, b = int(toff[v]), int(toff[v + 1])
+        k = int(nin[v])
+        assert sorted(touch[a:a + k].tolist()) == sorted(s["ctouch"][a:a + k].tolist())
+        assert sorted(touch[a + k:b].tolist()) == sorted(s["ctouch"][a + k:b].tolist())
