@@ -1157,6 +1157,57 @@ __global__ void k_set_rank(const u32 *__restrict__ mv, const u32 *__restrict__ d
     if (i < *dM) rank[mv[i]] = i;
 }
 
+// k-way pair ranking (include/axc.h AXC_PAIR_RANK_MAX_K): the moves, in (gain desc, id asc)
+// order, get the key of their direction group: (min(p,q) * K + max(p,q)) * 2 + (p > q).
+constexpr u32 PAIR_RANK_MAX_K = AXC_PAIR_RANK_MAX_K;
+__global__ void k_pair_group(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ part,
+                             const u32 *__restrict__ target, u32 K, u32 *__restrict__ gk, u32 *__restrict__ pos) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *dM) return;
+    const u32 u = mv[i], p = part[u], q = target[u];
+    gk[i] = (((p < q ? p : q) * K + (p < q ? q : p)) << 1) | (p < q ? 0u : 1u);
+    pos[i] = i;
+}
+__device__ __forceinline__ u32 lower_bound_u32(const u32 *a, u32 n, u32 x) {
+    u32 lo = 0, hi = n;
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+// After the stable sort by group key: the move at position j is the i-th of its group; the i-th of
+// the opposite direction is its partner. Pair gain into psn[node] (indexed by node, so later
+// passes can rebuild the key after any permutation), (pair position << 1 | d) into k1.
+__global__ void k_pair_keys(const u32 *__restrict__ gk, const u32 *__restrict__ pos, const u32 *__restrict__ dM,
+                            const u32 *__restrict__ mv, const i64 *__restrict__ gain, i64 *__restrict__ psn,
+                            u32 *__restrict__ k1, u32 *__restrict__ node) {
+    const u32 M = *dM, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= M) return;
+    const u32 g = gk[j], d = g & 1u;
+    const u32 i = j - lower_bound_u32(gk, M, g);
+    const u32 s2 = lower_bound_u32(gk, M, g ^ 1u), e2 = lower_bound_u32(gk, M, (g ^ 1u) + 1u);
+    const u32 u = mv[pos[j]];
+    i64 ps = gain[u];
+    u32 pk = j;
+    if (i < e2 - s2) {
+        ps += gain[mv[pos[s2 + i]]];
+        if (d) pk = s2 + i;
+    }
+    psn[u] = ps;
+    k1[j] = (pk << 1) | d;
+    node[j] = u;
+}
+// Descending pair-gain keys of the permuted movers (hi and lo words of pbound - ps).
+__global__ void k_pair_gain_keys(const u32 *__restrict__ node, const u32 *__restrict__ dM, const i64 *__restrict__ psn,
+                                 u64 pbound, u32 *__restrict__ hi, u32 *__restrict__ lo) {
+    const u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= *dM) return;
+    const u64 k = pbound - (u64)psn[node[j]];
+    hi[j] = (u32)(k >> 32);
+    lo[j] = (u32)k;
+}
+
 // ------------------------------------------------------------------ cascade
 constexpr u32 CC_WARPS = 4;
 constexpr u32 CC_MOV = 128;    // movers per hyperedge handled by the warp kernel
@@ -1640,14 +1691,6 @@ __global__ void k_size_delta(const u32 *__restrict__ mv, const u32 *__restrict__
     u32 ev = val[i];
     i64 s = nsize[mv[ev >> 1]];
     d[i] = (ev & 1) ? s : -s;
-}
-__device__ __forceinline__ u32 lower_bound_u32(const u32 *a, u32 len, u32 x) {
-    u32 lo = 0, hi = len;
-    while (lo < hi) {
-        u32 mid = (lo + hi) >> 1;
-        if (a[mid] < x) lo = mid + 1; else hi = mid;
-    }
-    return lo;
 }
 __global__ void k_size_flags(const u32 *__restrict__ key, const u32 *__restrict__ val, const i64 *__restrict__ d,
                              const i64 *__restrict__ E, const u32 *__restrict__ dne, const u64 *__restrict__ psize,
@@ -2183,6 +2226,24 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         radix_sort_pairs_dn(c, khi, mv, dM, n, kb - 32);
     } else {
         radix_sort_pairs_dn(c, klo, mv, dM, n, kb);
+    }
+    if (!rp.encourage && rp.K <= PAIR_RANK_MAX_K) {  // k-way: moves in p <-> q pairs
+        u32 *gk = khi, *pos = klo;  // the gain keys are spent
+        LAUNCH(c, k_pair_group, cdiv(n, 256), 256, 0, mv, dM, part, target, rp.K, gk, pos);
+        radix_sort_pairs_dn(c, gk, pos, dM, n, bits_for(2 * (u64)rp.K * rp.K));
+        i64 *psn = c.arena.alloc<i64>(n);
+        u32 *k1 = c.arena.alloc<u32>(n), *node = c.arena.alloc<u32>(n);
+        LAUNCH(c, k_pair_keys, cdiv(n, 256), 256, 0, gk, pos, dM, mv, gain, psn, k1, node);
+        radix_sort_pairs_dn(c, k1, node, dM, n, bits_for(2 * (u64)n));
+        const u64 pbound = 2 * lp.gain_bound;
+        const u32 pb = bits_for(pbound);
+        LAUNCH(c, k_pair_gain_keys, cdiv(n, 256), 256, 0, node, dM, psn, pbound, khi, klo);
+        radix_sort_pairs_dn(c, klo, node, dM, n, pb < 32 ? pb : 32);
+        if (pb > 32) {
+            LAUNCH(c, k_pair_gain_keys, cdiv(n, 256), 256, 0, node, dM, psn, pbound, khi, klo);
+            radix_sort_pairs_dn(c, khi, node, dM, n, pb - 32);
+        }
+        AXC_CUDA(cudaMemcpyAsync(mv, node, (size_t)n * 4, cudaMemcpyDeviceToDevice, c.stream));
     }
     LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank, dSE);
     // cascade

@@ -132,6 +132,10 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the sampler's start-up takes a host core for a moment; let it pass before timing
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self

@@ -95,6 +95,11 @@ typedef struct {
 #define AXC_SPARSE_GAIN_K 4096u
 #define AXC_SPARSE_GAIN_SAMPLE 4096u
 #define AXC_SPARSE_GAIN_CANDIDATES 8u
+/* k-way refinement orders its moves in pairs: the i-th best move from partition a to b next to the
+ * i-th best from b to a, pairs ranked by their summed gain, so that balanced prefixes exist when
+ * every partition is near its size limit (the reference's chaining, sources/chaining.cu:19-254,
+ * serves the same purpose). Up to this many partitions; above it moves are ranked by gain. */
+#define AXC_PAIR_RANK_MAX_K 32768u
 
 typedef struct {
     uint32_t num_parts;        /* K' after zero-basing */

@@ -30,6 +30,7 @@ typedef uint64_t u64;
 typedef int64_t i64;
 const u32 NONE = 0xFFFFFFFFu;
 const u64 RATE_MAX_LEN = AXC_RATE_MAX_LEN;  // the rating's hyperedge length limit (include/axc.h)
+const u32 PAIR_RANK_MAX_K = AXC_PAIR_RANK_MAX_K;  // k-way pair ranking needs (a*K + b) * 2 < 2^32
 
 struct G {
     u32 n = 0, e = 0;
@@ -489,6 +490,47 @@ std::vector<u64> part_inbound(const Census &cs, u32 e, u32 K) {
     return pi;
 }
 
+// k-way move order (this build's deterministic stand-in for the reference's chaining,
+// sources/chaining.cu:19-254, which links a move into partition q with a move out of q so that
+// prefixes stay balanced). mv arrives in (gain desc, id asc) order. Moves between the same two
+// partitions a < b are split by direction d (0: a -> b, 1: b -> a); the i-th move of one
+// direction (in that order) pairs with the i-th of the other. A pair is ranked by the sum of its
+// two gains, a single by its own gain; ties by the pair's position (a, b, i), and d = 0 first,
+// so the two moves of a pair are adjacent and every even prefix of a pair chain is balanced.
+void pair_rank(const std::vector<u32> &part, const std::vector<u32> &target, const std::vector<i64> &gain,
+               std::vector<u32> &mv, u32 K) {
+    const size_t M = mv.size();
+    std::vector<u32> gk(M), ord(M);
+    for (size_t i = 0; i < M; ++i) {
+        const u32 p = part[mv[i]], q = target[mv[i]];
+        gk[i] = ((std::min(p, q) * K + std::max(p, q)) << 1) | (p < q ? 0u : 1u);
+    }
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(), [&](u32 x, u32 y) { return gk[x] < gk[y]; });
+    std::vector<u32> sk(M);
+    for (size_t j = 0; j < M; ++j) sk[j] = gk[ord[j]];
+    struct Key { i64 ps; u64 pk; u32 u; };
+    std::vector<Key> keys(M);
+    for (size_t j = 0; j < M; ++j) {
+        const u32 g = sk[j], d = g & 1u;
+        const size_t s = std::lower_bound(sk.begin(), sk.end(), g) - sk.begin(), i = j - s;
+        const size_t s2 = std::lower_bound(sk.begin(), sk.end(), g ^ 1u) - sk.begin();
+        const size_t e2 = std::upper_bound(sk.begin(), sk.end(), g ^ 1u) - sk.begin();
+        const u32 u = mv[ord[j]];
+        i64 ps = gain[u];
+        u64 pk = j;
+        if (i < e2 - s2) {
+            ps += gain[mv[ord[s2 + i]]];
+            if (d == 1) pk = s2 + i;
+        }
+        keys[j] = {ps, (pk << 1) | d, u};
+    }
+    std::stable_sort(keys.begin(), keys.end(), [](const Key &x, const Key &y) {
+        return x.ps != y.ps ? x.ps > y.ps : x.pk < y.pk;
+    });
+    for (size_t j = 0; j < M; ++j) mv[j] = keys[j].u;
+}
+
 // One refinement round (sources/refinement.cu:82-543 restated with exact integers):
 // proposals -> rank by (gain desc, id asc) -> cascaded gain of each move assuming every
 // better-ranked move is applied (per hyperedge sweep) -> prefix sums -> size excess and inbound
@@ -508,6 +550,7 @@ bool refine_round(const RefineCtx &rc, std::vector<u32> &part, u32 discount, u32
         if (target[u] != NONE) mv.push_back(u);
     if (mv.empty()) return false;
     std::stable_sort(mv.begin(), mv.end(), [&](u32 a, u32 b) { return gain[a] > gain[b]; });
+    if (!rc.encourage && rc.K <= PAIR_RANK_MAX_K) pair_rank(part, target, gain, mv, rc.K);
     const u32 M = (u32)mv.size();
     std::vector<u32> rank(g.n, NONE);
     for (u32 r = 0; r < M; ++r) rank[mv[r]] = r;
