@@ -25,7 +25,7 @@ RATE_MAX_LEN = 128  # AXC_RATE_MAX_LEN: longer hyperedges take no part in the ra
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error", 4: "I/O error",
     5: "malformed input", 6: "infeasible", 7: "timed out", 8: "unknown job", 9: "admission refused",
-    10: "internal device check failed", 11: "size exceeds limit",
+    10: "internal device check failed", 11: "size exceeds limit", 12: "canceled at shutdown",
 }
 
 
@@ -81,7 +81,7 @@ EXPORTS = [
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
     "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
-    "axc_serve_configure",
+    "axc_serve_configure", "axc_selftest_bounded_wait",
 ]
 
 _lib = None
@@ -207,6 +207,21 @@ def write(path: str, g: Hypergraph) -> None:
     rc = lib().axc_write_hgraph(path.encode(), C.byref(g.c()))
     if rc:
         raise AxcError(rc)
+
+
+def read_partition(path: str, n: int) -> np.ndarray:
+    """HyperGraph::loadPartitioning (includes/hgraph.hpp:1062-1083): n partition ids."""
+    out = np.zeros(max(n, 1), np.uint32)
+    rc = lib().axc_read_partition(path.encode(), n, _ptr(out, C.c_uint32))
+    if rc:
+        raise AxcError(rc, path)
+    return out[:n]
+
+
+def quotient(g: Hypergraph, part: np.ndarray) -> Hypergraph:
+    """The quotient hypergraph of `-s` built on the host (axc_quotient_hgraph)."""
+    part = np.ascontiguousarray(part, dtype=np.uint32)
+    return _owned(lib().axc_quotient_hgraph, C.byref(g.c()), _ptr(part, C.c_uint32))
 
 
 def gen_snn(layers, width, fanout, sigma=0.0, cap=0, p_next=1.0, seed=0) -> Hypergraph:

@@ -144,7 +144,9 @@ struct Executor {
         return AXC_OK;
     }
 
-    ~Executor() {
+    // Stops the lanes after their running jobs, answers every job still queued with
+    // AXC_ECANCELED and wakes its pollers. Idempotent.
+    void shutdown() {
         {
             std::lock_guard<std::mutex> lk(mu);
             stop = true;
@@ -152,23 +154,37 @@ struct Executor {
         cv_work.notify_all();
         for (auto &t : threads)
             if (t.joinable()) t.join();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (Job *j : queue) {
+                j->rc = AXC_ECANCELED;
+                j->err = "the context shut down before the job ran";
+                j->done = true;
+            }
+            queue.clear();
+        }
+        cv_done.notify_all();
         for (Lane *l : lanes) lane_destroy(l);
+        lanes.clear();
     }
+
+    ~Executor() { shutdown(); }
 };
 
-// per-context executor, created at the first submit with the configured lanes and budget
+// per-context executor, created at the first submit with the configured lanes and budget; held
+// by shared_ptr so that a poller waiting on it keeps it alive while the context shuts down
 static std::mutex g_mu;
-static std::map<axc_ctx *, std::unique_ptr<Executor>> g_exec;
+static std::map<axc_ctx *, std::shared_ptr<Executor>> g_exec;
 static std::map<axc_ctx *, std::pair<uint32_t, size_t>> g_config;
 
-static Executor *executor_for(axc_ctx *ctx, int *rc) {
+static std::shared_ptr<Executor> executor_for(axc_ctx *ctx, int *rc) {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_exec.find(ctx);
     if (it != g_exec.end()) {
         *rc = AXC_OK;
-        return it->second.get();
+        return it->second;
     }
-    auto x = std::make_unique<Executor>();
+    auto x = std::make_shared<Executor>();
     auto cfg = g_config.find(ctx);
     x->nlanes = cfg != g_config.end() ? cfg->second.first : 1;
     size_t budget = cfg != g_config.end() ? cfg->second.second : 0;
@@ -177,9 +193,8 @@ static Executor *executor_for(axc_ctx *ctx, int *rc) {
     if (const char *e = std::getenv("AXC_SERVE_EXCLUSIVE_PINS")) x->excl_pins = std::strtoull(e, nullptr, 10);
     *rc = x->start(ctx_device(ctx));
     if (*rc) return nullptr;
-    Executor *p = x.get();
-    g_exec[ctx] = std::move(x);
-    return p;
+    g_exec[ctx] = x;
+    return x;
 }
 
 }  // namespace axc
@@ -187,7 +202,7 @@ static Executor *executor_for(axc_ctx *ctx, int *rc) {
 using namespace axc;
 
 extern "C" void axc_batch_free(axc_ctx *ctx) {
-    std::unique_ptr<Executor> e;
+    std::shared_ptr<Executor> e;
     {
         std::lock_guard<std::mutex> lk(g_mu);
         g_config.erase(ctx);
@@ -196,7 +211,7 @@ extern "C" void axc_batch_free(axc_ctx *ctx) {
         e = std::move(it->second);
         g_exec.erase(it);
     }
-    e.reset();  // joins the lane threads
+    e->shutdown();  // joins the lane threads, cancels queued jobs, wakes their pollers
 }
 
 extern "C" int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_budget) {
@@ -232,10 +247,11 @@ extern "C" int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p
     j->est = estimate_bytes(g);
     j->pins = P;
     int rc = AXC_OK;
-    Executor *x = executor_for(ctx, &rc);
+    std::shared_ptr<Executor> x = executor_for(ctx, &rc);
     if (!x) return rc;
     {
         std::lock_guard<std::mutex> lk(x->mu);
+        if (x->stop) return AXC_ECANCELED;
         j->id = x->next_id++;
         *job_id = j->id;
         x->queue.push_back(j.get());
@@ -248,7 +264,7 @@ extern "C" int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p
 extern "C" int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms) {
     if (!ctx) return AXC_EINVAL;
     int rc = AXC_OK;
-    Executor *x = executor_for(ctx, &rc);
+    std::shared_ptr<Executor> x = executor_for(ctx, &rc);  // kept alive while this call waits
     if (!x) return rc;
     std::unique_lock<std::mutex> lk(x->mu);
     auto it = x->jobs.find(job_id);

@@ -261,6 +261,9 @@ void scan_excl_u32(Ctx &c, const u32 *in, u32 *out, u64 n);
 void scan_excl_u64(Ctx &c, const u64 *in, u64 *out, u64 n);
 void scan_excl_i64(Ctx &c, const i64 *in, i64 *out, u64 n);
 void scan_incl_i64(Ctx &c, const i64 *in, i64 *out, u64 n);
+// one look-back wait on a tile flag that nothing publishes, polled spin_limit times (the
+// failure path of the scans' bounded waits); throws AXC_EINTERNAL when it gave up
+void lookback_selftest(Ctx &c, u32 spin_limit);
 // Tile state of the single-pass scans (made by axc_create, freed by axc_destroy).
 void scan_state_create(Ctx &c, u32 cap_tiles);
 void scan_state_destroy(Ctx &c);

@@ -147,7 +147,7 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
             deep_part = c.arena.alloc<u32>(cur.n ? cur.n : 1);
             kway_initial(c, cur, R.k, deep_part);
             K = R.k;
-            refine_deepest = true;
+            refine_deepest = !kway_multistart(c, cur, wfx, R.k, R.omega, R.seed, deep_part);
             break;
         }
         const size_t tmp = c.arena.mark();
@@ -165,7 +165,7 @@ static u32 partition_core(Ctx &c, u32 n, u32 e, const u64 *d_off, const u32 *d_p
             deep_part = c.arena.alloc<u32>(cur.n ? cur.n : 1);
             kway_initial(c, cur, R.k, deep_part);
             K = R.k;
-            refine_deepest = true;
+            refine_deepest = !kway_multistart(c, cur, wfx, R.k, R.omega, R.seed, deep_part);
             break;
         }
         if (!R.kway && (ng <= R.target || ng == cur.n || (l >= 32 && ratio > 0.95f))) {
@@ -246,6 +246,7 @@ const char *axc_strerror(int s) {
         case AXC_EBUSY: return "admission refused by the memory budget";
         case AXC_EINTERNAL: return "internal device check failed";
         case AXC_EOVERFLOW: return "size exceeds the limit of this call";
+        case AXC_ECANCELED: return "the context shut down before the job ran";
         default: return "unknown status";
     }
 }
@@ -841,6 +842,19 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
     } catch (const std::exception &e) {
         cudaStreamSynchronize(c.stream);
         c.arena.release(0);
+        return guard(ctx, e);
+    }
+}
+
+int axc_selftest_bounded_wait(axc_ctx *ctx, uint32_t spin_limit) {
+    if (!ctx || spin_limit == 0) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Ctx &c = ctx->c;
+    try {
+        lookback_selftest(c, spin_limit);
+        return AXC_OK;
+    } catch (const std::exception &e) {
+        cudaStreamSynchronize(c.stream);
         return guard(ctx, e);
     }
 }

@@ -49,6 +49,9 @@ struct RefineParams {
     bool encourage;
     u32 rounds;
     u64 seed;
+    // copies > 1: the level is that many disjoint copies of copy_n nodes each (the k-way
+    // multi-start); moves are ranked copy by copy and every copy takes its own best prefix
+    u32 copies = 1, copy_n = 0;
 };
 void setup_refine_kernels(Ctx &c);
 // all refinement rounds of one level; part[n] is updated in place; returns rounds applied
@@ -78,6 +81,9 @@ void part_inbound(Ctx &c, const DLevel &L, const Census &cs, u64 *pinb, u32 K);
 
 // initpart.cu
 void kway_initial(Ctx &c, const DLevel &L, u32 k, u32 *part);
+// the k-way multi-start on the coarsest level (include/axc.h AXC_KWAY_TRIES): refines part[n]
+// from its BFS start and random ones, keeps the best; false when fewer than 2 copies fit
+bool kway_multistart(Ctx &c, const DLevel &L, const u32 *wfx, u32 k, u32 omega, u64 seed, u32 *part);
 
 // post.cu
 u32 greedy_pack(Ctx &c, const u64 *ss, const u64 *si, u32 m, u64 omega, u64 delta, u32 *packid);

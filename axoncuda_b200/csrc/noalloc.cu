@@ -9,7 +9,6 @@
 //            used for hyperedges longer than NA_SMEM_LEN; cleared by the block before each use
 // Hyperedges longer than NA_MAX_LEN are refused (AXC_EOVERFLOW).
 #include <algorithm>
-#include <mutex>
 
 #include "common.cuh"
 
@@ -78,9 +77,9 @@ __global__ void __launch_bounds__(256) k_na_small(u32 e, const u64 *__restrict__
         const i64 l = __popc(__ballot_sync(0xFFFFFFFFu, first));
         if (lane == 0) {
             const i64 wf = na_weight(w, h);
-            conn += wf * (l - 1);
+            conn += wf * (l > 0 ? l - 1 : 0);  // an empty hyperedge connects nothing
             cut += l > 1 ? wf : 0;
-            soed += wf * (l - 1) * (i64)len;
+            soed += wf * (l > 0 ? l - 1 : 0) * (i64)len;
         }
     }
     conn = warp_sum(conn);
@@ -128,9 +127,9 @@ __global__ void __launch_bounds__(256) k_na_large(u32 e, const u64 *__restrict__
         __syncthreads();
         if (threadIdx.x == 0) {
             const i64 wf = na_weight(w, h), l = distinct;
-            conn += wf * (l - 1);
+            conn += wf * (l > 0 ? l - 1 : 0);  // an empty hyperedge connects nothing
             cut += l > 1 ? wf : 0;
-            soed += wf * (l - 1) * (i64)len;
+            soed += wf * (l > 0 ? l - 1 : 0) * (i64)len;
         }
         __syncthreads();
     }
@@ -140,22 +139,11 @@ __global__ void __launch_bounds__(256) k_na_large(u32 e, const u64 *__restrict__
     }
 }
 
-// Device address of the scratch array, looked up once per device with that device current.
-std::mutex g_na_mu;
-u32 *g_na_ptr[256] = {};
-
-cudaError_t na_scratch(int dev, u32 **out) {
-    std::lock_guard<std::mutex> lk(g_na_mu);
-    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
-    if (!g_na_ptr[dev]) {
-        u32 *ptr = nullptr;
-        cudaError_t rc = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
-        if (rc != cudaSuccess) return rc;
-        g_na_ptr[dev] = ptr;
-    }
-    *out = g_na_ptr[dev];
-    return cudaSuccess;
-}
+// Device address of the scratch array in the current context. A symbol's address belongs to a
+// context, not to a device ordinal: after cudaDeviceReset, or under a driver-API context that the
+// caller made current, an address cached by device would be stale. The lookup allocates nothing,
+// so it is made on every call.
+cudaError_t na_scratch(u32 **out) { return cudaGetSymbolAddress((void **)out, g_noalloc_scratch); }
 
 }  // namespace
 }  // namespace axc
@@ -166,10 +154,8 @@ extern "C" int axc_connectivity_noalloc(uint32_t e, const uint64_t *d_hedge_off,
                                         const float *d_hedge_w, const uint32_t *d_part, void *stream,
                                         int64_t *out_fx) {
     if (!out_fx || (e && (!d_hedge_off || !d_pins || !d_part))) return AXC_EINVAL;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return AXC_ECUDA;
     u32 *scratch = nullptr;
-    if (na_scratch(dev, &scratch) != cudaSuccess) return AXC_ECUDA;
+    if (na_scratch(&scratch) != cudaSuccess) return AXC_ECUDA;
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(scratch, 0, NA_HEADER_WORDS * 4, s) != cudaSuccess) return AXC_ECUDA;
     if (e) {

@@ -83,9 +83,10 @@ __global__ void k_metrics(u32 e, const u64 *__restrict__ off, const u32 *__restr
         const i64 w = wfx[h];
         const i64 l = lam[h];
         const i64 len = (i64)(off[h + 1] - off[h]);
-        conn = w * (l - 1);
+        const i64 l1 = l > 0 ? l - 1 : 0;  // an empty hyperedge connects nothing
+        conn = w * l1;
         cut = l > 1 ? w : 0;
-        soed = w * (l - 1) * len;
+        soed = w * l1 * len;
     }
     conn = warp_sum(conn);
     cut = warp_sum(cut);

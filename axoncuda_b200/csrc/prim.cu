@@ -125,7 +125,8 @@ __device__ __forceinline__ void lb_leave(const ScanState &S, u32 epoch) {
 // tile publishes its aggregate, then (after looking back over its predecessors with warp 0) its
 // inclusive prefix. Returns the exclusive prefix of the tile to every thread.
 template <class TO>
-__device__ TO lookback_prefix(const ScanState &S, u32 epoch, u32 t, TO tile_total, u32 *status, TO *s_prefix) {
+__device__ TO lookback_prefix(const ScanState &S, u32 epoch, u32 t, TO tile_total, u32 *status, TO *s_prefix,
+                              u32 spin_limit = LB_SPIN_LIMIT) {
     const u32 lane = threadIdx.x & 31u;
     if (threadIdx.x == 0) {
         if (t == 0) {
@@ -151,7 +152,7 @@ __device__ TO lookback_prefix(const ScanState &S, u32 epoch, u32 t, TO tile_tota
                 for (u32 it = 0;; ++it) {
                     f = ld_flag(&S.flag[idx]);
                     if ((f >> 2) == epoch && (f & 3u)) break;
-                    if (it >= LB_SPIN_LIMIT) {
+                    if (it >= spin_limit) {
                         gave_up = true;
                         f = (epoch << 2) | 2u;
                         break;
@@ -279,6 +280,15 @@ void scan_impl(Ctx &c, const TI *in, TO *out, u64 n, const u32 *skip_n = nullptr
     scan_impl<TO, TO>(c, part, part, tiles);
     LAUNCH(c, (k_tile_scan<TI, TO>), tiles, SCAN_THREADS, 0, in, out, (const TO *)part, n);
     c.arena.release(m);
+}
+
+// The bounded wait of the look-back, made to run out: the block plays tile 1 of epoch 1 in a
+// private tile state whose tile 0 never publishes, so its warp polls that flag `spin_limit` times,
+// gives up, sets the status word and returns.
+__global__ void k_lookback_selftest(ScanState S, u32 *status, u32 spin_limit, u64 *out) {
+    __shared__ u64 s_prefix;
+    const u64 p = lookback_prefix<u64>(S, 1u, 1u, 5ull, status, &s_prefix, spin_limit);
+    if (threadIdx.x == 0) *out = p;
 }
 
 __global__ void k_offsets_tail(const u32 *counts, u64 *out, u64 n) {
@@ -494,6 +504,23 @@ void scan_excl_u32(Ctx &c, const u32 *in, u32 *out, u64 n) { scan_impl<u32, u32>
 void scan_excl_u64(Ctx &c, const u64 *in, u64 *out, u64 n) { scan_impl<u64, u64>(c, in, out, n); }
 void scan_excl_i64(Ctx &c, const i64 *in, i64 *out, u64 n) { scan_impl<i64, i64>(c, in, out, n); }
 void scan_incl_i64(Ctx &c, const i64 *in, i64 *out, u64 n) { scan_impl<i64, i64, true>(c, in, out, n); }
+
+void lookback_selftest(Ctx &c, u32 spin_limit) {
+    const size_t m = c.arena.mark();
+    ScanState S;
+    S.flag = c.arena.alloc<u32>(2);
+    S.agg = c.arena.alloc<u64>(2);
+    S.incl = c.arena.alloc<u64>(2);
+    S.ctrl = c.arena.alloc<u32>(4);
+    S.cap_tiles = 2;
+    u64 *out = c.arena.alloc<u64>(1);
+    AXC_CUDA(cudaMemsetAsync(S.flag, 0, 8, c.stream));
+    AXC_CUDA(cudaMemsetAsync(S.ctrl, 0, 16, c.stream));
+    LAUNCH(c, k_lookback_selftest, 1, 32, 0, S, c.d_status, spin_limit, out);
+    AXC_CUDA(cudaStreamSynchronize(c.stream));
+    c.arena.release(m);
+    check_status(c);  // throws AXC_EINTERNAL with the status word (DEV_SPIN_LIMIT) when the wait gave up
+}
 
 void setup_prim_kernels() {
     AXC_CUDA(cudaFuncSetAttribute(k_rs_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RSS_SMEM));

@@ -1830,6 +1830,53 @@ __global__ void k_apply(const u32 *__restrict__ mv, const u32 *__restrict__ targ
     part[v] = target[v];
 }
 
+// Copies (the k-way multi-start): moves are sorted by copy last, so every copy owns one rank
+// segment; ck[r] is the copy of rank r. One block per copy finds its segment's best prefix with
+// the prefix values taken relative to the segment start, and decides its own application.
+__global__ void k_copy_keys(const u32 *__restrict__ mv, const u32 *__restrict__ dM, u32 copy_n, u32 *__restrict__ ck) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < *dM) ck[i] = mv[i] / copy_n;
+}
+__global__ void k_best_seg(const i64 *__restrict__ pre, u32 n, int has_vi, const u32 *__restrict__ dM,
+                           const u32 *__restrict__ ck, Best *__restrict__ best, u32 *__restrict__ capply,
+                           u32 *__restrict__ apply) {
+    __shared__ Best sh[32];
+    const u32 M = *dM, t = blockIdx.x;
+    const u32 s = lower_bound_u32(ck, M, t), e = lower_bound_u32(ck, M, t + 1);
+    const i64 g0 = s ? seg_prefix(pre, n, 0, s - 1) : 0, v0 = s ? seg_prefix(pre, n, 1, s - 1) : 0;
+    const i64 i0 = (s && has_vi) ? seg_prefix(pre, n, 2, s - 1) : 0;
+    Best b{0, 0, 0, 0xFFFFFFFFu};
+    for (u32 r = s + threadIdx.x; r < e; r += blockDim.x) {
+        const u32 ok = has_vi ? (seg_prefix(pre, n, 2, r) - i0 == 0 ? 1u : 0u) : 1u;
+        Best c{ok, seg_prefix(pre, n, 1, r) - v0, seg_prefix(pre, n, 0, r) - g0, r};
+        b = best_pick(b, c);
+    }
+    b = warp_best_prefix(b);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        Best x = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : Best{0, 0, 0, 0xFFFFFFFFu};
+        x = warp_best_prefix(x);
+        if (threadIdx.x == 0) {
+            best[t] = x;
+            const i64 vi = (has_vi && x.r != 0xFFFFFFFFu) ? seg_prefix(pre, n, 2, x.r) - i0 : 0;
+            const u32 ap = (x.r != 0xFFFFFFFFu && x.vs <= 0 && vi <= 0 && x.g >= 0) ? 1u : 0u;
+            capply[t] = ap;
+            if (ap) atomicOr(apply, 1u);
+        }
+    }
+}
+__global__ void k_apply_seg(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ ck,
+                            const u32 *__restrict__ target, const Best *__restrict__ best,
+                            const u32 *__restrict__ capply, u32 *__restrict__ part) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *dM) return;
+    const u32 t = ck[i];
+    if (!capply[t] || i > best[t].r) return;
+    const u32 v = mv[i];
+    part[v] = target[v];
+}
+
 GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp, const Census &cs, const u32 *part,
                         const u64 *psize, const u64 *pinb, u32 discount, u32 round, u32 *target, i64 *gain,
                         u32 *status) {
@@ -2245,6 +2292,12 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         }
         AXC_CUDA(cudaMemcpyAsync(mv, node, (size_t)n * 4, cudaMemcpyDeviceToDevice, c.stream));
     }
+    u32 *ck = nullptr;  // copies: the copy of every rank, ascending
+    if (rp.copies > 1) {
+        ck = c.arena.alloc<u32>(n);
+        LAUNCH(c, k_copy_keys, cdiv(n, 256), 256, 0, mv, dM, rp.copy_n, ck);
+        radix_sort_pairs_dn(c, ck, mv, dM, n, bits_for(rp.copies - 1));
+    }
     LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank, dSE);
     // cascade
 
@@ -2346,11 +2399,19 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     }
     scan_incl_i64(c, raw, pre, 3 * (u64)n);
     // best prefix and apply
-    const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
-    Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
-    LAUNCH(c, k_best, nbk, 256, 0, pre, n, track ? 1 : 0, dM, bb + 1);
-    LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, pre, n, track ? 1 : 0, bb, apply);
-    LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
+    if (rp.copies > 1) {  // every copy its own
+        Best *bs = (Best *)c.arena.alloc<u64>(4 * (u64)rp.copies);
+        u32 *capply = c.arena.alloc<u32>(rp.copies);
+        AXC_CUDA(cudaMemsetAsync(apply, 0, 4, c.stream));
+        LAUNCH(c, k_best_seg, rp.copies, 256, 0, pre, n, track ? 1 : 0, dM, ck, bs, capply, apply);
+        LAUNCH(c, k_apply_seg, cdiv(n, 256), 256, 0, mv, dM, ck, target, bs, capply, part);
+    } else {
+        const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
+        Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
+        LAUNCH(c, k_best, nbk, 256, 0, pre, n, track ? 1 : 0, dM, bb + 1);
+        LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, pre, n, track ? 1 : 0, bb, apply);
+        LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
+    }
     c.arena.release(keep);
     return apply;
 }

@@ -42,7 +42,8 @@ typedef enum {
     AXC_ENOTFOUND = 8,     /* unknown job id */
     AXC_EBUSY = 9,         /* admission refused (memory budget) */
     AXC_EINTERNAL = 10,    /* device-side invariant check failed (status word set by a kernel) */
-    AXC_EOVERFLOW = 11     /* a size exceeds the documented limit of the call */
+    AXC_EOVERFLOW = 11,    /* a size exceeds the documented limit of the call */
+    AXC_ECANCELED = 12     /* the context shut down before the submitted job ran */
 } axc_status;
 
 typedef enum { AXC_MODE_INCC = 0, AXC_MODE_KWAY = 1 } axc_mode;
@@ -100,6 +101,15 @@ typedef struct {
  * every partition is near its size limit (the reference's chaining, sources/chaining.cu:19-254,
  * serves the same purpose). Up to this many partitions; above it moves are ranked by gain. */
 #define AXC_PAIR_RANK_MAX_K 32768u
+/* k-way initial partition: a multi-start on the coarsest level, in place of the reference's
+ * Mt-KaHyPar call (sources/init_part.cu:733-953) and in the manner of its dormant GPU routine
+ * (32 random starts with refinement, sources/init_part.cu:186-727). Up to AXC_KWAY_TRIES starts
+ * (the BFS chunks and random balanced ones), as many as fit AXC_KWAY_TRY_PINS pins in all, are
+ * refined together for AXC_KWAY_TRY_ROUNDS rounds as disjoint copies of the level; the one of
+ * least connectivity is kept. With fewer than 2 copies the BFS chunks are refined alone. */
+#define AXC_KWAY_TRIES 16u
+#define AXC_KWAY_TRY_ROUNDS 32u
+#define AXC_KWAY_TRY_PINS 16777216ull
 
 typedef struct {
     uint32_t num_parts;        /* K' after zero-basing */
@@ -234,7 +244,8 @@ int axc_gen_circuit(uint32_t n, uint32_t e, uint32_t smin, uint32_t smax, double
  * half the free device memory at the first submit. */
 int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_budget);
 int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint64_t *job_id);
-/* Wait up to timeout_ms (<0: forever) for a job; copies its partition into out_part[n]. */
+/* Wait up to timeout_ms (<0: forever) for a job; copies its partition into out_part[n]. A job
+ * still queued when the context is destroyed is answered with AXC_ECANCELED. */
 int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms);
 /* Partition `count` jobs through the same lanes (submit all, then wait for all). out_parts[i]
  * points at a host buffer of g[i].n entries; stats may be NULL. Returns the first failing status. */
@@ -285,6 +296,15 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
                     const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage,
                     uint32_t discount, uint32_t *out_target, int64_t *out_gain);
 
+/* ---- failure path of the bounded device waits (no reference counterpart: the reference's waits
+ * are grid syncs and host synchronizations, which never time out) ------------------------------------
+ * Runs one look-back wait of the single-pass scans (the only waits on other blocks' flags in this
+ * library) against a tile flag that nothing publishes, polling it spin_limit times (the scans poll
+ * 2^24 times). The wait gives up, the kernel sets the status word and returns, and the call reports
+ * AXC_EINTERNAL with the status in axc_last_error; the context stays usable. Returns AXC_OK only
+ * if the wait did not give up, which would be a defect. */
+int axc_selftest_bounded_wait(axc_ctx *ctx, uint32_t spin_limit);
+
 /* ---- connectivity without allocating (no reference counterpart) ---------------------------------
  * out_fx[0..2] = connectivity_fx, cutnet_fx and soed_fx of part[] over a hypergraph already in
  * device memory, equal to what axc_evaluate reports for the same inputs. For callers that may not
@@ -295,7 +315,9 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
  * array that must start at zero on every call.
  * - Runs on the current device, on `stream` (a cudaStream_t; NULL = the default stream), and
  *   synchronizes that stream before returning.
- * - The first call on each device looks up the scratch address; make that call before any stream
+ * - Every call looks up the scratch array's address in the current context (a lookup, no
+ *   allocation), so it follows cudaDeviceReset and contexts the caller makes current. The first
+ *   call in a context may load the library's device code; make that call before any stream
  *   capture.
  * - Hyperedges longer than 16384 pins are refused with AXC_EOVERFLOW; a partition id of
  *   UINT32_MAX gives AXC_EINVAL.

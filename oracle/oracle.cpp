@@ -321,6 +321,9 @@ struct RefineCtx {
     u32 K, omega, delta;
     bool encourage;
     u64 seed;
+    // copies > 1: the level is that many disjoint copies of copy_n nodes each (the k-way
+    // multi-start); moves are ranked copy by copy and every copy takes its own best prefix
+    u32 copies = 1, copy_n = 0;
 };
 
 inline i64 leave_gain(bool encourage, u32 w, u32 c) {
@@ -551,6 +554,8 @@ bool refine_round(const RefineCtx &rc, std::vector<u32> &part, u32 discount, u32
     if (mv.empty()) return false;
     std::stable_sort(mv.begin(), mv.end(), [&](u32 a, u32 b) { return gain[a] > gain[b]; });
     if (!rc.encourage && rc.K <= PAIR_RANK_MAX_K) pair_rank(part, target, gain, mv, rc.K);
+    if (rc.copies > 1)
+        std::stable_sort(mv.begin(), mv.end(), [&](u32 a, u32 b) { return a / rc.copy_n < b / rc.copy_n; });
     const u32 M = (u32)mv.size();
     std::vector<u32> rank(g.n, NONE);
     for (u32 r = 0; r < M; ++r) rank[mv[r]] = r;
@@ -631,21 +636,35 @@ bool refine_round(const RefineCtx &rc, std::vector<u32> &part, u32 discount, u32
             Vi[r] = v;
         }
     }
-    u32 best = 0;
-    for (u32 r = 1; r < M; ++r) {
-        const u32 a = best, b = r;
-        const bool aok = Vi[a] == 0, bok = Vi[b] == 0;
-        bool take;
-        if (aok != bok) take = bok;
-        else if (!aok) take = false;
-        else if (Vs[a] != Vs[b]) take = Vs[a] > Vs[b];
-        else if (G2[a] != G2[b]) take = G2[a] < G2[b];
-        else take = false;
-        if (take) best = b;
+    // best prefix of every copy's rank segment [s, e) (one segment without copies), prefix values
+    // relative to the segment start
+    bool any = false;
+    for (u32 s = 0; s < M;) {
+        u32 e = s + 1;
+        if (rc.copies > 1)
+            while (e < M && mv[e] / rc.copy_n == mv[s] / rc.copy_n) ++e;
+        else
+            e = M;
+        auto rel = [&](const std::vector<i64> &X, u32 r) { return X[r] - (s ? X[s - 1] : 0); };
+        u32 best = s;
+        for (u32 r = s + 1; r < e; ++r) {
+            const u32 a = best, b = r;
+            const bool aok = rel(Vi, a) == 0, bok = rel(Vi, b) == 0;
+            bool take;
+            if (aok != bok) take = bok;
+            else if (!aok) take = false;
+            else if (rel(Vs, a) != rel(Vs, b)) take = rel(Vs, a) > rel(Vs, b);
+            else if (rel(G2, a) != rel(G2, b)) take = rel(G2, a) < rel(G2, b);
+            else take = false;
+            if (take) best = b;
+        }
+        if (rel(Vs, best) <= 0 && rel(Vi, best) <= 0 && rel(G2, best) >= 0) {
+            for (u32 r = s; r <= best; ++r) part[mv[r]] = target[mv[r]];
+            any = true;
+        }
+        s = e;
     }
-    if (!(Vs[best] <= 0 && Vi[best] <= 0 && G2[best] >= 0)) return false;
-    for (u32 r = 0; r <= best; ++r) part[mv[r]] = target[mv[r]];
-    return true;
+    return any;
 }
 
 void refine_level(const RefineCtx &rc, std::vector<u32> &part, u32 R) {
@@ -727,6 +746,74 @@ std::vector<u32> kway_initial(const G &g, const T &t, const u32 *nsize, u32 k) {
         before += nsize[v];
     }
     return part;
+}
+
+// A random balanced start of the k-way multi-start: nodes ordered by
+// (mix32(v ^ mix32(t * 0x9E3779B9 + seed)), v), cut into weight chunks as kway_initial does.
+std::vector<u32> kway_random(const G &g, const u32 *nsize, u32 k, u32 t, u64 seed) {
+    const u32 salt = mix32(t * 0x9E3779B9u + (u32)seed);
+    std::vector<u32> ord(g.n), key(g.n), part(g.n, 0);
+    for (u32 v = 0; v < g.n; ++v) key[v] = mix32(v ^ salt);
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(), [&](u32 a, u32 b) { return key[a] < key[b]; });
+    u64 W = 0;
+    for (u32 v = 0; v < g.n; ++v) W += nsize[v];
+    u64 before = 0;
+    for (u32 i = 0; i < g.n; ++i) {
+        const u32 v = ord[i];
+        const u64 x = (2 * before + nsize[v]) * (u64)k / (2 * (W ? W : 1));
+        part[v] = (u32)std::min<u64>(x, k - 1);
+        before += nsize[v];
+    }
+    return part;
+}
+
+// The k-way multi-start on the coarsest level (include/axc.h AXC_KWAY_TRIES): T copies of the
+// level without its hyperedges of fewer than 2 pins (they never change a k-way gain), copy 0
+// starting from `part`, copy t >= 1 from kway_random(t); all refined together for
+// AXC_KWAY_TRY_ROUNDS rounds (each copy takes its own best prefix); the copy of least
+// connectivity (the first on ties) replaces `part`. Returns false when fewer than 2 copies fit.
+bool kway_multistart(const G &g, const std::vector<u32> &wfx, const u32 *nsize, u32 k, u32 omega, u64 seed,
+                     std::vector<u32> &part) {
+    std::vector<u32> keep;
+    u64 P2 = 0;
+    for (u32 h = 0; h < g.e; ++h) {
+        const u64 len = g.off[h + 1] - g.off[h];
+        if (len >= 2) { keep.push_back(h); P2 += len; }
+    }
+    const u64 NC = P2 ? std::min<u64>(AXC_KWAY_TRIES, AXC_KWAY_TRY_PINS / P2) : 0;
+    if (NC < 2) return false;
+    const u32 n = g.n, e2 = (u32)keep.size();
+    G S;
+    S.n = (u32)(NC * n);
+    S.e = (u32)(NC * e2);
+    S.off.assign(1, 0);
+    std::vector<u32> wS;
+    for (u32 t = 0; t < NC; ++t)
+        for (u32 h : keep) {
+            for (u64 i = g.off[h]; i < g.off[h + 1]; ++i) S.pins.push_back(g.pins[i] + t * n);
+            S.off.push_back(S.pins.size());
+            S.nsrc.push_back(g.nsrc[h]);
+            wS.push_back(wfx[h]);
+        }
+    T tS = touching(S);
+    std::vector<u32> nsS((size_t)NC * n), pS((size_t)NC * n);
+    for (u32 t = 0; t < NC; ++t) {
+        std::vector<u32> p0 = t == 0 ? part : kway_random(g, nsize, k, t, seed);
+        for (u32 v = 0; v < n; ++v) { nsS[(size_t)t * n + v] = nsize[v]; pS[(size_t)t * n + v] = p0[v] + t * k; }
+    }
+    RefineCtx rc{&S, &tS, &wS, nsS.data(), (u32)(NC * k), omega, 0x7FFFFFFFu, false, seed};
+    rc.copies = (u32)NC;
+    rc.copy_n = n;
+    refine_level(rc, pS, AXC_KWAY_TRY_ROUNDS);
+    Census cs = census(S, pS);
+    std::vector<i64> conn(NC, 0);
+    for (u32 h = 0; h < S.e; ++h) conn[h / e2] += (i64)wS[h] * (i64)(cs.beg[h + 1] - cs.beg[h] - 1);
+    u32 best = 0;
+    for (u32 t = 1; t < NC; ++t)
+        if (conn[t] < conn[best]) best = t;
+    for (u32 v = 0; v < n; ++v) part[v] = pS[(size_t)best * n + v] - best * k;
+    return true;
 }
 
 struct Level {
@@ -933,9 +1020,10 @@ void or_evaluate(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pi
             if (k >= s && mkd[p] != h) { mkd[p] = h; inb[p]++; }
         }
         const i64 wf = (i64)or_wfx(w ? w[h] : 1.0f);
-        conn += wf * (i64)(lam - 1);
+        const i64 l1 = lam ? (i64)lam - 1 : 0;  // an empty hyperedge connects nothing
+        conn += wf * l1;
         cut += lam > 1 ? wf : 0;
-        soed += wf * (i64)(lam - 1) * (i64)(b - a);
+        soed += wf * l1 * (i64)(b - a);
     }
     u64 mi = 0;
     for (u32 p = 0; p < K; ++p) mi = std::max(mi, inb[p]);
@@ -977,7 +1065,8 @@ uint32_t or_partition(uint32_t n, uint32_t e, const uint64_t *off, const uint32_
         const u32 cn = cur.g.n;
         if (kway && cn < 8192) {
             cpart = kway_initial(cur.g, cur.t, cur.nsize.data(), k);
-            K = k; refine_deepest = true;
+            K = k;
+            refine_deepest = !kway_multistart(cur.g, wfx, cur.nsize.data(), k, omega, seed, cpart);
             break;
         }
         std::vector<u32> pairs((size_t)cn * cnc), scores((size_t)cn * cnc), groups(cn);
@@ -988,7 +1077,8 @@ uint32_t or_partition(uint32_t n, uint32_t e, const uint64_t *off, const uint32_
         const float ratio = (float)ng / (float)cn;
         if (kway && (ratio > 0.95f || ng < 1024)) {
             cpart = kway_initial(cur.g, cur.t, cur.nsize.data(), k);
-            K = k; refine_deepest = true;
+            K = k;
+            refine_deepest = !kway_multistart(cur.g, wfx, cur.nsize.data(), k, omega, seed, cpart);
             break;
         }
         if (!kway && (ng <= target || ng == cn || (lv >= 32 && ratio > 0.95f))) {

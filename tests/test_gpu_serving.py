@@ -72,3 +72,37 @@ def test_configure_after_start_is_refused():
         with pytest.raises(ax.AxcError) as e:
             srv.serve_configure(4, 1 << 30)
         assert e.value.code == 9  # AXC_EBUSY
+
+
+def test_destroy_answers_waiting_pollers():
+    """Destroying a serving context while jobs are queued: the running job finishes, every queued
+    job is answered with AXC_ECANCELED, and pollers already waiting (timeout -1) return instead of
+    waiting for good."""
+    import ctypes as C
+    import threading
+    import time
+    g = ax.gen_snn(10, 4000, 64, 0.0, 0, 1.0, 77)  # 2.3M pins: each job runs alone on the device
+    p = ax.params_kway(8, 0.03, cnc=4, rfr=8)
+    srv = ax.Context(0, 256 << 20)
+    srv.serve_configure(1, 8 << 30)
+    ids = [srv.submit(g, p) for _ in range(12)]
+    rcs, entered = {}, [threading.Event() for _ in range(3)]
+    bufs = [np.zeros(g.n, np.uint32) for _ in range(3)]
+
+    def wait(i):
+        h = srv._h  # NULL once the context is closed: axc_poll would then say AXC_EINVAL
+        entered[i].set()
+        rcs[i] = ax.lib().axc_poll(h, ids[9 + i], bufs[i].ctypes.data_as(C.POINTER(C.c_uint32)), None, -1)
+
+    threads = [threading.Thread(target=wait, args=(i,)) for i in range(3)]
+    for t in threads:
+        t.start()
+    for e in entered:
+        assert e.wait(30)
+    time.sleep(0.05)  # the pollers are inside axc_poll, waiting
+    srv.close()  # axc_destroy: shuts the executor down
+    for t in threads:
+        t.join(timeout=120)
+        assert not t.is_alive()
+    assert all(rc in (0, 12) for rc in rcs.values()), rcs  # AXC_OK or AXC_ECANCELED
+    assert 12 in rcs.values()  # the last jobs were still queued behind the running one
