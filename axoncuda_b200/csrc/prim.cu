@@ -3,6 +3,7 @@
 // with warp-level match_any ranking, fills and reductions. Every launch goes through the
 // context's stream.
 #include "common.cuh"
+#include "blocksort.cuh"
 
 namespace axc {
 
@@ -414,82 +415,17 @@ __global__ void k_compact_write(const u32 *flags, const u32 *pos, u32 *out, u64 
 }
 
 // ------------------------------------------------------------------ small radix sort
-// Arrays of at most RSS_CAP elements sort in one block: every 8-bit pass in shared memory, one
-// launch for the whole sort. Warp w owns elements [w*256, (w+1)*256) in 8 rounds of 32, so the
-// ranks (digit offset + earlier warps' counts + match_any rank in the warp) keep the sort stable.
-constexpr int RSS_WARPS = 32;
-constexpr int RSS_ITEMS = 8;
-constexpr int RSS_CAP = RSS_WARPS * 32 * RSS_ITEMS;  // 8192
-constexpr size_t RSS_SMEM = (size_t)4 * RSS_CAP * 4 + (size_t)RSS_WARPS * 256 * 4 + 257 * 4;
-
+// Arrays of at most RSS_CAP elements sort in one block (blocksort.cuh): every 8-bit pass in
+// shared memory, one launch for the whole sort.
 __global__ void __launch_bounds__(RSS_WARPS * 32) k_rs_small(u32 *__restrict__ keys, u32 *__restrict__ vals, u32 n_cap,
                                                              const u32 *__restrict__ d_n, u32 bits) {
     extern __shared__ u32 sm[];
-    u32 *ka = sm, *va = ka + RSS_CAP, *kb = va + RSS_CAP, *vb = kb + RSS_CAP;
-    u32 *wcnt = vb + RSS_CAP;         // [RSS_WARPS][256]
-    u32 *dbase = wcnt + RSS_WARPS * 256;  // [257]
     if (d_n && *d_n > n_cap) return;  // more than one block holds: the multi-pass sort takes it
     const u32 n = d_n ? *d_n : n_cap;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (u32 i = threadIdx.x; i < n; i += blockDim.x) { ka[i] = keys[i]; va[i] = vals[i]; }
-    const u32 lt = (1u << lane) - 1u;
-    for (u32 shift = 0; shift < bits; shift += 8) {
-        for (int i = threadIdx.x; i < RSS_WARPS * 256; i += blockDim.x) wcnt[i] = 0;
-        __syncthreads();
-        u32 dig[RSS_ITEMS], loc[RSS_ITEMS];
-#pragma unroll
-        for (int r = 0; r < RSS_ITEMS; ++r) {
-            const u32 i = (u32)w * 32 * RSS_ITEMS + (u32)r * 32 + lane;
-            const bool ok = i < n;
-            const u32 d = ok ? ((ka[i] >> shift) & 255u) : 256u;
-            dig[r] = d;
-            const u32 peers = __match_any_sync(0xFFFFFFFFu, d);
-            const u32 before = ok ? wcnt[w * 256 + d] : 0u;
-            loc[r] = before + __popc(peers & lt);
-            __syncwarp();
-            if (ok && (peers & lt) == 0) wcnt[w * 256 + d] = before + __popc(peers);
-            __syncwarp();
-        }
-        __syncthreads();
-        // per digit: counts over warps -> running offsets; then digit bases by a scan over 256
-        if (threadIdx.x < 256) {
-            const u32 d = threadIdx.x;
-            u32 run = 0;
-            for (int ww = 0; ww < RSS_WARPS; ++ww) {
-                const u32 t = wcnt[ww * 256 + d];
-                wcnt[ww * 256 + d] = run;
-                run += t;
-            }
-            dbase[d] = run;
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {  // exclusive scan of the 256 digit totals, 8 per lane
-            u32 v[8], s = 0;
-            for (int k = 0; k < 8; ++k) { v[k] = dbase[lane * 8 + k]; s += v[k]; }
-            u32 x = s;
-            for (int o = 1; o < 32; o <<= 1) {
-                const u32 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if (lane >= o) x += y;
-            }
-            u32 pre = x - s;
-            for (int k = 0; k < 8; ++k) { dbase[lane * 8 + k] = pre; pre += v[k]; }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < RSS_ITEMS; ++r) {
-            const u32 d = dig[r];
-            if (d < 256u) {
-                const u32 i = (u32)w * 32 * RSS_ITEMS + (u32)r * 32 + lane;
-                const u32 pos = dbase[d] + wcnt[w * 256 + d] + loc[r];
-                kb[pos] = ka[i];
-                vb[pos] = va[i];
-            }
-        }
-        __syncthreads();
-        u32 *t = ka; ka = kb; kb = t;
-        t = va; va = vb; vb = t;
-    }
-    for (u32 i = threadIdx.x; i < n; i += blockDim.x) { keys[i] = ka[i]; vals[i] = va[i]; }
+    for (u32 i = threadIdx.x; i < n; i += blockDim.x) { sm[i] = keys[i]; sm[RSS_CAP + i] = vals[i]; }
+    const u32 *ko, *vo;
+    block_radix_sort(sm, n, bits, ko, vo);
+    for (u32 i = threadIdx.x; i < n; i += blockDim.x) { keys[i] = ko[i]; vals[i] = vo[i]; }
 }
 
 inline u32 grid_for(Ctx &c, u64 n, u32 threads = 256) {

@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "blocksort.cuh"
 
 namespace axc {
 namespace {
@@ -1226,6 +1227,10 @@ struct CascadeArgs {
     int32_t *tdv;
     u32 *dT;
     u64 tcap;
+    // when set (small levels), transitions are summed per (partition, rank) instead: entry
+    // p * dense_stride + r gets ((d << 32) + 1) per transition, its count below and its net above
+    unsigned long long *tdense;
+    u32 dense_stride;
     u32 *status;
     u32 K;  // partitions: with K <= CC_DIRECT_K the per-hyperedge tables are indexed by partition id
 };
@@ -1248,6 +1253,10 @@ __device__ __forceinline__ void cascade_fill(const CascadeArgs &A, u64 a, u32 lm
 }
 
 __device__ __forceinline__ void emit_at(const CascadeArgs &A, u32 s, u32 p, u32 r, int32_t d) {
+    if (A.tdense) {
+        atomicAdd(&A.tdense[(u64)p * A.dense_stride + r], ((unsigned long long)(i64)d << 32) + 1ull);
+        return;
+    }
     if (s >= A.tcap) { atomicExch(A.status, DEV_BAD_INDEX); return; }
     A.tp[s] = p;
     A.tr[s] = r;
@@ -1755,6 +1764,90 @@ __global__ void k_trans_flags(const u32 *__restrict__ sp, const u32 *__restrict_
     if (was_bad != is_bad) atomicAdd(&Vi[sr[j]], (unsigned long long)(i64)(is_bad ? 1 : -1));
 }
 
+// ---- size and inbound validity of every prefix on small levels: one block per partition ----------
+// The same quantities as the event pipelines above (k_size_events ... k_size_flags and
+// k_trans_keys ... k_trans_flags), without sorting: a partition's size events are its movers in
+// rank order, and its inbound transitions arrive summed per rank (CascadeArgs::tdense).
+//  - sizes: Vs[r] += excess(after rank r) - excess(before), excess = max(size - omega, 0);
+//  - inbound: Vi[r] += bad(after r) - bad(before r) at each rank with transitions, bad = the
+//    running inbound count above delta, and "before" taken as good at the partition's first
+//    such rank (kernels/refinement.cu:632-651). Both telescope over the events of one rank, so
+//    the order of events within a rank does not matter.
+constexpr u32 VS_THREADS = 1024;
+constexpr u32 VS_MAX_K = 256;    // partitions (blocks)
+
+__device__ __forceinline__ i64 block_incl_scan_i64(i64 v, i64 *sh, i64 &total) {
+    const u32 lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const i64 y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if ((int)lane >= o) v += y;
+    }
+    __syncthreads();
+    if (lane == 31) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        i64 x = lane < (blockDim.x >> 5) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const i64 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        sh[lane] = x;  // inclusive warp prefixes
+    }
+    __syncthreads();
+    total = sh[(blockDim.x >> 5) - 1];
+    return v + (w ? sh[w - 1] : 0);
+}
+__global__ void __launch_bounds__(VS_THREADS) k_validity_small(
+    const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ part,
+    const u32 *__restrict__ target, const u32 *__restrict__ nsize, const u64 *__restrict__ psize, u64 omega,
+    unsigned long long *__restrict__ Vs, int track, const unsigned long long *__restrict__ tdense, u32 stride,
+    const u64 *__restrict__ pinb, u64 delta, unsigned long long *__restrict__ Vi) {
+    __shared__ i64 sh[32];
+    const u32 p = blockIdx.x, M = *dM;
+    i64 run = (i64)psize[p];
+    const i64 om = (i64)omega;
+    for (u32 base = 0; base < M; base += VS_THREADS) {
+        const u32 r = base + threadIdx.x;
+        i64 d = 0;
+        if (r < M) {
+            const u32 v = mv[r];
+            if (part[v] == p) d = -(i64)nsize[v];
+            else if (target[v] == p) d = (i64)nsize[v];
+        }
+        i64 tot;
+        const i64 incl = block_incl_scan_i64(d, sh, tot);
+        if (d != 0) {
+            const i64 after = run + incl, before = after - d;
+            const i64 dx = (after > om ? after - om : 0) - (before > om ? before - om : 0);
+            if (dx) atomicAdd(&Vs[r], (unsigned long long)dx);
+        }
+        run += tot;
+    }
+    if (!track) return;
+    const i64 dl = (i64)delta;
+    i64 run2 = (i64)pinb[p];
+    bool seen = false;  // a rank with transitions of p came before this chunk
+    for (u32 base = 0; base < M; base += VS_THREADS) {
+        const u32 r = base + threadIdx.x;
+        const unsigned long long x = r < M ? tdense[(u64)p * stride + r] : 0ull;
+        const bool has = (u32)x != 0u;
+        const i64 D = has ? (i64)(int32_t)(u32)(x >> 32) : 0;
+        i64 tot, htot;
+        const i64 incl = block_incl_scan_i64(D, sh, tot);
+        const i64 hincl = block_incl_scan_i64(has ? 1 : 0, sh, htot);
+        if (has) {
+            const i64 after = run2 + incl, before = after - D;
+            const bool first = !seen && hincl == 1;
+            const bool bad_before = !first && before > dl, bad_after = after > dl;
+            if (bad_before != bad_after) atomicAdd(&Vi[r], (unsigned long long)(i64)(bad_after ? 1 : -1));
+        }
+        run2 += tot;
+        seen = seen || htot > 0;
+    }
+}
+
 // best prefix (best_move_functor): inbound-valid first, then fewer size violations, then larger
 // gain, then the earlier rank.
 struct Best {
@@ -1786,6 +1879,127 @@ __device__ __forceinline__ Best warp_best_prefix(Best b) {
     }
     return b;
 }
+// ---- small levels (n <= RSS_CAP): ranking, and prefix sums + best prefix + apply, one block each ----
+// The movers in id order, ranked by (gain desc, id asc): compaction by block scans, the stable
+// radix sort of the descending gain keys (a second pass over the high words when the gain bound
+// needs more than 32 bits), then the ranks. Also resets every node's rank and cascaded gain and
+// writes the mover count and the size-event count, as k_move_flags ... k_set_rank do.
+__global__ void __launch_bounds__(RSS_WARPS * 32) k_rank_small(u32 n, const u32 *__restrict__ target,
+                                                              const i64 *__restrict__ gain, u64 gbound, u32 kb,
+                                                              u32 *__restrict__ mv, u32 *__restrict__ rank,
+                                                              unsigned long long *__restrict__ g2, u32 *__restrict__ dM,
+                                                              u32 *__restrict__ twice) {
+    extern __shared__ u32 sm[];
+    __shared__ i64 sh[32];
+    u32 M = 0;
+    for (u32 b = 0; b < n; b += blockDim.x) {
+        const u32 v = b + threadIdx.x;
+        const bool f = v < n && target[v] != NONE;
+        if (v < n) { rank[v] = NONE; g2[v] = 0; }
+        i64 tot;
+        const i64 incl = block_incl_scan_i64(f ? 1 : 0, sh, tot);
+        if (f) {
+            const u32 pos = M + (u32)incl - 1;
+            sm[pos] = (u32)(gbound - (u64)gain[v]);
+            sm[RSS_CAP + pos] = v;
+        }
+        M += (u32)tot;
+    }
+    const u32 *ko, *vo;
+    block_radix_sort(sm, M, kb < 32 ? kb : 32, ko, vo);
+    if (kb > 32) {  // high words of the movers in their low-word order
+        u32 hv[RSS_ITEMS], nv[RSS_ITEMS];
+#pragma unroll
+        for (int k = 0; k < RSS_ITEMS; ++k) {
+            const u32 i = threadIdx.x + (u32)k * blockDim.x;
+            nv[k] = i < M ? vo[i] : 0u;
+            hv[k] = i < M ? (u32)((gbound - (u64)gain[nv[k]]) >> 32) : 0u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < RSS_ITEMS; ++k) {
+            const u32 i = threadIdx.x + (u32)k * blockDim.x;
+            if (i < M) { sm[i] = hv[k]; sm[RSS_CAP + i] = nv[k]; }
+        }
+        block_radix_sort(sm, M, kb - 32, ko, vo);
+    }
+    for (u32 i = threadIdx.x; i < M; i += blockDim.x) {
+        const u32 v = vo[i];
+        mv[i] = v;
+        rank[v] = i;
+    }
+    if (threadIdx.x == 0) {
+        *dM = M;
+        *twice = 2 * M;
+    }
+}
+
+// The inclusive prefix sums by rank of the cascaded gains, size violations (Vs) and inbound
+// violations (Vi), the best prefix by best_better, and its application when it is valid with a
+// non-negative gain: k_gather_g2, the 3n scan, k_best, k_best_final and k_apply in one block.
+__global__ void __launch_bounds__(1024) k_tail_small(const u32 *__restrict__ mv, const u32 *__restrict__ dM,
+                                                     const unsigned long long *__restrict__ g2,
+                                                     const i64 *__restrict__ Vs, const i64 *__restrict__ Vi, int has_vi,
+                                                     const u32 *__restrict__ target, u32 *__restrict__ part,
+                                                     u32 *__restrict__ apply) {
+    __shared__ i64 sh[32];
+    __shared__ Best bsh[32];
+    __shared__ i64 vsh[32];
+    __shared__ Best s_best;
+    __shared__ i64 s_vi;
+    const u32 M = *dM, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) { s_best = Best{0, 0, 0, 0xFFFFFFFFu}; s_vi = 0; }
+    i64 rg = 0, rs = 0, ri = 0;
+    for (u32 base = 0; base < M; base += blockDim.x) {
+        const u32 r = base + threadIdx.x;
+        const bool in = r < M;
+        i64 tg, ts, ti;
+        const i64 pg = rg + block_incl_scan_i64(in ? (i64)g2[mv[r]] : 0, sh, tg);
+        const i64 ps = rs + block_incl_scan_i64(in ? Vs[r] : 0, sh, ts);
+        const i64 pi = ri + block_incl_scan_i64(in ? Vi[r] : 0, sh, ti);
+        Best b{has_vi ? (pi == 0 ? 1u : 0u) : 1u, ps, pg, in ? r : 0xFFFFFFFFu};
+        i64 bvi = pi;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            Best c;
+            c.ok = __shfl_xor_sync(0xFFFFFFFFu, b.ok, o);
+            c.vs = __shfl_xor_sync(0xFFFFFFFFu, b.vs, o);
+            c.g = __shfl_xor_sync(0xFFFFFFFFu, b.g, o);
+            c.r = __shfl_xor_sync(0xFFFFFFFFu, b.r, o);
+            const i64 cvi = __shfl_xor_sync(0xFFFFFFFFu, bvi, o);
+            const Best x = best_pick(b, c);
+            if (x.r != b.r) bvi = cvi;
+            b = x;
+        }
+        if (lane == 0) { bsh[w] = b; vsh[w] = bvi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            Best x = s_best;
+            i64 xv = s_vi;
+            for (u32 k = 0; k < blockDim.x / 32; ++k) {
+                const Best y = best_pick(x, bsh[k]);
+                if (y.r != x.r) xv = vsh[k];
+                x = y;
+            }
+            s_best = x;
+            s_vi = xv;
+        }
+        rg += tg;
+        rs += ts;
+        ri += ti;
+    }
+    __syncthreads();
+    const Best x = s_best;
+    const i64 vi = has_vi ? s_vi : 0;
+    const bool ok = x.r != 0xFFFFFFFFu && x.vs <= 0 && vi <= 0 && x.g >= 0;
+    if (threadIdx.x == 0) *apply = ok ? 1u : 0u;
+    if (!ok) return;
+    for (u32 i = threadIdx.x; i <= x.r; i += blockDim.x) {
+        const u32 v = mv[i];
+        part[v] = target[v];
+    }
+}
+
 // best_better is a strict total order (ties end on the rank), so the tree reduction picks the
 // same prefix as a sequential scan would.
 // pre = inclusive scan of [gain deltas | size-violation deltas | inbound-violation deltas] by rank,
@@ -1930,6 +2144,7 @@ void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
     AXC_CUDA(cudaFuncSetAttribute(k_cascade_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_DYN_MAX));
     AXC_CUDA(cudaFuncSetAttribute(k_gain_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM));
+    AXC_CUDA(cudaFuncSetAttribute(k_rank_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RSS_SMEM));
 }
 
 __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
@@ -2256,13 +2471,18 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     u32 *cnt = c.arena.alloc<u32>(8);
     AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
     u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4;
+    // small levels: ranking, validity and the best prefix in one block each (SMALL_*)
+    const bool small = rp.K <= VS_MAX_K && n <= (u32)RSS_CAP && rp.copies == 1;
     // movers in id order, then ranked by (gain desc, id asc)
     u32 *flag = c.arena.alloc<u32>(n), *mv = c.arena.alloc<u32>(n), *rank = c.arena.alloc<u32>(n);
     unsigned long long *g2 = c.arena.alloc<unsigned long long>(n);  // cascaded gains, zeroed here
-    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag, rank, g2);
-    compact_indices_dn(c, flag, mv, n, dM);
     const u32 kb = bits_for(lp.gain_bound);
     u32 *khi = c.arena.alloc<u32>(n), *klo = c.arena.alloc<u32>(n);
+    if (small) {
+        LAUNCH(c, k_rank_small, 1, RSS_WARPS * 32, RSS_SMEM, n, target, gain, lp.gain_bound, kb, mv, rank, g2, dM, dSE);
+    } else {
+    LAUNCH(c, k_move_flags, cdiv(n, 256), 256, 0, n, target, flag, rank, g2);
+    compact_indices_dn(c, flag, mv, n, dM);
     LAUNCH(c, k_move_keys, cdiv(n, 256), 256, 0, mv, dM, gain, lp.gain_bound, khi, klo);
     if (kb > 32) {
         // stable by the low word, then by the high word (a 64-bit LSD sort); the high words are
@@ -2274,7 +2494,9 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     } else {
         radix_sort_pairs_dn(c, klo, mv, dM, n, kb);
     }
-    if (!rp.encourage && rp.K <= PAIR_RANK_MAX_K) {  // k-way: moves in p <-> q pairs
+    }
+    const bool pairs = !rp.encourage && rp.K <= PAIR_RANK_MAX_K;
+    if (pairs) {  // k-way: moves in p <-> q pairs
         u32 *gk = khi, *pos = klo;  // the gain keys are spent
         LAUNCH(c, k_pair_group, cdiv(n, 256), 256, 0, mv, dM, part, target, rp.K, gk, pos);
         radix_sort_pairs_dn(c, gk, pos, dM, n, bits_for(2 * (u64)rp.K * rp.K));
@@ -2298,15 +2520,21 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         LAUNCH(c, k_copy_keys, cdiv(n, 256), 256, 0, mv, dM, rp.copy_n, ck);
         radix_sort_pairs_dn(c, ck, mv, dM, n, bits_for(rp.copies - 1));
     }
-    LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank, dSE);
+    if (!small || pairs || rp.copies > 1) LAUNCH(c, k_set_rank, cdiv(n, 256), 256, 0, mv, dM, rank, dSE);
     // cascade
 
     // inbound-set transitions (INCC): each destination pin of a mover gives at most two
     const bool track = rp.delta < 0x7FFFFFFFu && lp.dst_pins;
-    const u64 tcap = track ? 2 * lp.dst_pins : 0;
+    // small levels check every prefix with one block per partition (k_validity_small), the
+    // transitions summed per (partition, rank) in a dense K x n table
+    const u64 tcap = track && !small ? 2 * lp.dst_pins : 0;
     u32 *tp = nullptr, *tr = nullptr;
     int32_t *tdv = nullptr;
-    if (track) {
+    unsigned long long *tdense = nullptr;
+    if (track && small) {
+        tdense = c.arena.alloc<unsigned long long>((u64)rp.K * n);
+        AXC_CUDA(cudaMemsetAsync(tdense, 0, (size_t)rp.K * n * 8, c.stream));
+    } else if (track) {
         tp = c.arena.alloc<u32>(tcap);
         tr = c.arena.alloc<u32>(tcap);
         tdv = (int32_t *)c.arena.alloc<u32>(tcap);
@@ -2317,6 +2545,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         C.wfx = wfx; C.lam = cs.lam; C.cpart = cs.part; C.ccnt = cs.cnt; C.cdcnt = cs.dcnt; C.rank = rank;
         C.part = part; C.target = target; C.g2 = g2;
         C.track = track ? 1 : 0; C.tp = tp; C.tr = tr; C.tdv = tdv; C.dT = dT; C.tcap = tcap;
+        C.tdense = tdense; C.dense_stride = n;
         C.status = c.d_status;
         C.K = rp.K;
         const bool direct = rp.K <= CC_DIRECT_K;
@@ -2358,9 +2587,18 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     // one buffer [G | Vs | Vi] so one inclusive scan makes all three prefix sums
     i64 *raw = c.arena.alloc<i64>(3 * (u64)n), *pre = c.arena.alloc<i64>(3 * (u64)n);
     i64 *Gx = raw, *Vs = raw + n, *Vi = raw + 2 * (u64)n;
+    if (small) {
+        AXC_CUDA(cudaMemsetAsync(Vs, 0, 2 * (size_t)n * 8, c.stream));  // Vs and Vi
+        LAUNCH(c, k_validity_small, rp.K, VS_THREADS, 0, mv, dM, part, target, L.nsize, psize, (u64)rp.omega,
+               (unsigned long long *)Vs, track ? 1 : 0, tdense, n, pinb, (u64)rp.delta, (unsigned long long *)Vi);
+        LAUNCH(c, k_tail_small, 1, 1024, 0, mv, dM, (const unsigned long long *)g2, Vs, Vi, track ? 1 : 0, target,
+               part, apply);
+        c.arena.release(keep);
+        return apply;
+    }
     LAUNCH(c, k_gather_g2, cdiv(n, 256), 256, 0, mv, dM, n, g2, Gx);  // also zeroes Vs and Vi
     // size validity
-    {
+    if (!small) {
         size_t m1 = c.arena.mark();
         const u32 nemax = 2 * n;
         u32 *key = c.arena.alloc<u32>(nemax), *val = c.arena.alloc<u32>(nemax);
@@ -2375,7 +2613,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     }
     // inbound validity (INCC only): the transitions ordered by (partition, rank), the running
     // inbound-set size of each partition along them
-    if (track) {
+    if (track && !small) {
         size_t m1 = c.arena.mark();
         const u64 nt = tcap;
         const u32 rb = bits_for(n ? n - 1 : 0), pb = bits_for(rp.K ? rp.K - 1 : 0);
@@ -2465,6 +2703,31 @@ static u32 rg_kernels(cudaGraph_t g) {
     return kernels;
 }
 
+// The round schedule on the device, for the level's rounds run as the body of one conditional
+// WHILE graph node. rs = {r, R, rounds done}; after each round: the next r by the skip rule after
+// a round without moves (sources/refinement.cu:539-542; the host loop of refine_level is the same
+// rule), its discount (1, 2, none by thirds) and round number into dyn, and the loop goes on while
+// r < R and the status word is clear.
+__global__ void k_round_next(cudaGraphConditionalHandle h, u32 *__restrict__ rs, u32 *__restrict__ dyn,
+                             const u32 *__restrict__ apply, const u32 *__restrict__ status) {
+    u32 r = rs[0];
+    const u32 R = rs[1];
+    rs[2] += 1;
+    if (!*apply) {
+        if (r < R / 3) r = R / 2;
+        else if (r < 2 * R / 3) r = 2 * R / 3;
+        else r = R;
+    }
+    r += 1;
+    rs[0] = r;
+    const bool go = r < R && *(volatile const u32 *)status == 0;
+    if (go) {
+        dyn[0] = r < R / 3 ? 1u : (r < 2 * R / 3 ? 2u : 0xFFFFFFFFu);
+        dyn[1] = r;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 // level bounds that need the offsets: the largest hyperedge and the destination pin count
 __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ nsrc,
                                unsigned long long *__restrict__ out) {
@@ -2482,6 +2745,72 @@ __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__
     }
 }
 
+// All rounds of a level in one graph launch: a conditional WHILE node whose body is one round
+// (round_body) followed by k_round_next, which applies the round schedule on the device. Returns
+// the rounds run.
+static u32 refine_level_loop(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
+                             u32 *part) {
+    const u32 R = rp.rounds;
+    u32 *dyn = c.arena.alloc<u32>(2), *rs = c.arena.alloc<u32>(4);
+    {
+        u32 *hp = (u32 *)((char *)c.h_pinned + 64);
+        hp[0] = 1u;  // discount of round 0 (R >= 2, so round 0 is in the first third)
+        hp[1] = 0u;
+        hp[2] = 0u;  // rs: r, R, rounds done
+        hp[3] = R;
+        hp[4] = 0u;
+        hp[5] = 0u;
+        AXC_CUDA(cudaMemcpyAsync(dyn, hp, 8, cudaMemcpyHostToDevice, c.stream));
+        AXC_CUDA(cudaMemcpyAsync(rs, hp + 2, 16, cudaMemcpyHostToDevice, c.stream));
+    }
+    RoundGraph rg;
+    AXC_CUDA(cudaGraphCreate(&rg.g, 0));
+    cudaGraphConditionalHandle h;
+    AXC_CUDA(cudaGraphConditionalHandleCreate(&h, rg.g, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    AXC_CUDA(cudaGraphAddNode(&wn, rg.g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const size_t m1 = c.arena.mark();
+    const u32 launches0 = c.launches;
+    size_t keep;
+    u32 *apply = nullptr;
+    AXC_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    c.capturing = true;
+    try {
+        apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep);
+        LAUNCH(c, k_round_next, 1, 1, 0, h, rs, dyn, apply, c.d_status);
+    } catch (...) {
+        c.capturing = false;
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c.stream, &junk);
+        throw;
+    }
+    c.capturing = false;
+    AXC_CUDA(cudaStreamEndCapture(c.stream, &body));
+    c.launches = launches0;
+    const u32 body_kernels = rg_kernels(body);
+    AXC_CUDA(cudaGraphInstantiate(&rg.x, rg.g, 0));
+    // the round's scratch above m1 stays unallocated, and nothing else allocates, while the graph runs
+    c.arena.release(m1);
+    AXC_CUDA(cudaGraphLaunch(rg.x, c.stream));
+    u32 *hp = (u32 *)((char *)c.h_pinned + 64);
+    AXC_CUDA(cudaMemcpyAsync(hp, rs, 16, cudaMemcpyDeviceToHost, c.stream));
+    AXC_CUDA(cudaMemcpyAsync(hp + 4, c.d_status, 4, cudaMemcpyDeviceToHost, c.stream));
+    AXC_CUDA(cudaStreamSynchronize(c.stream));
+    const u32 done = hp[2];
+    c.launches += done * body_kernels;
+    if (hp[4] != DEV_OK) {
+        AXC_CUDA(cudaMemsetAsync(c.d_status, 0, 4, c.stream));
+        throw Error(AXC_EINTERNAL, "device status word = " + std::to_string(hp[4]));
+    }
+    return done;
+}
+
 u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, u32 *part) {
     const u32 R = rp.rounds;
     if (R == 0 || L.n == 0) return 0;
@@ -2490,6 +2819,14 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
     // Graph replays need the round's scalars in device memory. Kernel-timer pairs captured in the
     // graph are read back after every replay; the bytes of the captured launches count per replay.
     const bool graph = R > 1;
+    // Without the kernel timer the rounds run as one conditional WHILE graph: the schedule lives
+    // on the device and the host waits once per level. With the timer on, each round is one replay
+    // of the round graph, so that its event pairs are read after every round.
+    if (graph && !c.prof_on) {
+        const u32 done = refine_level_loop(c, L, lp, wfx, rp, part);
+        c.arena.release(m);
+        return done;
+    }
     size_t ev0 = 0, ev1 = 0;
     u64 bytes_per_round = 0;
     RoundGraph rg;
