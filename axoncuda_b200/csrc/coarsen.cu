@@ -141,9 +141,10 @@ __device__ __forceinline__ u64 cand_key(const RateArgs &A, u32 u, u32 v, u32 s, 
 // the low word is the neighbour id; 0 is empty). One pass, so each neighbour's size and inbound
 // count are read once.
 // Inserts key k into the descending list top[0, cnc) (a key not above the last entry drops out).
-__device__ __forceinline__ void top_insert(u64 (&top)[AXC_MAX_CANDIDATES], u64 k, u32 cnc) {
+template <int TC>
+__device__ __forceinline__ void top_insert(u64 (&top)[TC], u64 k, u32 cnc) {
 #pragma unroll
-    for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
+    for (int i = 0; i < TC; ++i)
         if ((u32)i < cnc && k > top[i]) {
             const u64 t = top[i];
             top[i] = k;
@@ -151,11 +152,12 @@ __device__ __forceinline__ void top_insert(u64 (&top)[AXC_MAX_CANDIDATES], u64 k
         }
 }
 // Slots [first, cap) step `step` of the table, or with `used` the listed slots used[first, cap).
+template <int TC>
 __device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm,
-                                           u32 cap, u32 first, u32 step, u64 (&top)[AXC_MAX_CANDIDATES],
+                                           u32 cap, u32 first, u32 step, u64 (&top)[TC],
                                            const u32 *used = nullptr) {
 #pragma unroll
-    for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i) top[i] = 0;
+    for (int i = 0; i < TC; ++i) top[i] = 0;
     const u32 cnc = A.cnc;
     u64 floor = 0;  // the list's last entry: a key must beat it to enter
     for (u32 t = first; t < cap; t += step) {
@@ -164,18 +166,21 @@ __device__ __forceinline__ void top_collect(const RateArgs &A, u32 u, const u32 
         if (v == NONE) continue;
         const u64 k = cand_key(A, u, v, sc[s], cm[s]);
         if (k <= floor) continue;
-        top_insert(top, k, cnc);
+        top_insert<TC>(top, k, cnc);
 #pragma unroll
-        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i)
+        for (int i = 0; i < TC; ++i)
             if ((u32)i + 1 == cnc) floor = top[i];
     }
 }
-__device__ __forceinline__ void top_pop(u64 (&top)[AXC_MAX_CANDIDATES]) {
+template <int TC>
+__device__ __forceinline__ void top_pop(u64 (&top)[TC]) {
 #pragma unroll
-    for (int i = 0; i + 1 < (int)AXC_MAX_CANDIDATES; ++i) top[i] = top[i + 1];
-    top[AXC_MAX_CANDIDATES - 1] = 0;
+    for (int i = 0; i + 1 < TC; ++i) top[i] = top[i + 1];
+    top[TC - 1] = 0;
 }
 
+// TC: the length of the per-thread top lists, at least cnc (4 for cnc <= 4, else 16).
+template <int TC>
 __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u32 *__restrict__ list, u32 nlist) {
     __shared__ u32 tk[RT_WARPS][2 * RT_WARP_W], ts[RT_WARPS][2 * RT_WARP_W], tc[RT_WARPS][2 * RT_WARP_W];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -190,15 +195,15 @@ __global__ void __launch_bounds__(RT_WARPS * 32) k_rate_warp(RateArgs A, const u
     __syncwarp();
     rate_flat(A, u, keys, sc, cm, cap - 1, 0, 32);
     __syncwarp();
-    u64 top[AXC_MAX_CANDIDATES];
-    top_collect(A, u, keys, sc, cm, cap, lane, 32, top);
+    u64 top[TC];
+    top_collect<TC>(A, u, keys, sc, cm, cap, lane, 32, top);
     for (u32 r = 0; r < A.cnc; ++r) {
         const u64 best = warp_max_u64(top[0]);
         if (lane == 0) {
             A.pairs[(u64)u * A.cnc + r] = best ? (u32)best : NONE;
             A.scores[(u64)u * A.cnc + r] = best ? (u32)(best >> 32) : 0u;
         }
-        if (best && top[0] == best) top_pop(top);
+        if (best && top[0] == best) top_pop<TC>(top);
     }
 }
 
@@ -208,28 +213,29 @@ constexpr u32 RT_SEL = (RT_BLOCK / 32) * AXC_MAX_CANDIDATES;  // shared slots of
 // Each warp reduces its lanes' lists to its own top cnc with shuffles into red[warp * cnc ..];
 // warp 0 merges those after one barrier. red holds RT_SEL entries.
 // With `used`, only the nused listed slots are read.
+template <int TC>
 __device__ void rate_select(const RateArgs &A, u32 u, const u32 *keys, const u32 *sc, const u32 *cm, u32 cap,
                             u64 *red, const u32 *used = nullptr, u32 nused = 0) {
     const u32 lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5, cnc = A.cnc;
-    u64 top[AXC_MAX_CANDIDATES];
-    top_collect(A, u, keys, sc, cm, used ? nused : cap, threadIdx.x, blockDim.x, top, used);
+    u64 top[TC];
+    top_collect<TC>(A, u, keys, sc, cm, used ? nused : cap, threadIdx.x, blockDim.x, top, used);
     for (u32 r = 0; r < cnc; ++r) {
         const u64 best = warp_max_u64(top[0]);
         if (lane == 0) red[w * cnc + r] = best;
-        if (best && top[0] == best) top_pop(top);
+        if (best && top[0] == best) top_pop<TC>(top);
     }
     __syncthreads();
     if (w == 0) {
 #pragma unroll
-        for (int i = 0; i < (int)AXC_MAX_CANDIDATES; ++i) top[i] = 0;
-        for (u32 i = lane; i < nw * cnc; i += 32) top_insert(top, red[i], cnc);
+        for (int i = 0; i < TC; ++i) top[i] = 0;
+        for (u32 i = lane; i < nw * cnc; i += 32) top_insert<TC>(top, red[i], cnc);
         for (u32 r = 0; r < cnc; ++r) {
             const u64 best = warp_max_u64(top[0]);
             if (lane == 0) {
                 A.pairs[(u64)u * cnc + r] = best ? (u32)best : NONE;
                 A.scores[(u64)u * cnc + r] = best ? (u32)(best >> 32) : 0u;
             }
-            if (best && top[0] == best) top_pop(top);
+            if (best && top[0] == best) top_pop<TC>(top);
         }
     }
     __syncthreads();  // red is reused by the block's next node
@@ -247,6 +253,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_acc(RateArgs A, const u
     const u32 nw = blockDim.x >> 5;
     rate_flat(A, list[idx], keys, sc, cm, cap - 1, 32 * (s * nw + (threadIdx.x >> 5)), 32 * nw * splits);
 }
+template <int TC>
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, const u32 *__restrict__ list, u32 nl,
                                                                u32 cap, const u32 *gtab) {
     __shared__ u64 red[RT_SEL];
@@ -254,7 +261,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, cons
     if (idx >= nl) return;
     const u64 plane = (u64)nl * cap;
     const u32 *keys = gtab + (u64)idx * cap, *sc = keys + plane, *cm = sc + plane;
-    rate_select(A, list[idx], keys, sc, cm, cap, red);
+    rate_select<TC>(A, list[idx], keys, sc, cm, cap, red);
 }
 
 // One node per block iteration; table in dynamic smem (gtab == nullptr) or in this block's
@@ -265,6 +272,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_split_select(RateArgs A, cons
 // With `retry` set the launch is a first try on tables smaller than the nodes' work bounds: a node
 // whose distinct neighbours pass half of its table stops and is appended to retry / *d_retry.
 // With `d_nl` set the list length is read from device memory (at most nlist).
+template <int TC>
 __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *__restrict__ list, u32 nlist,
                                                         u32 cap_max, u32 *gtab, const u32 *__restrict__ d_nl,
                                                         u32 *__restrict__ retry, u32 *__restrict__ d_retry,
@@ -304,7 +312,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rate_block(RateArgs A, const u32 *
         if (retry && ndist > limit) {  // table too small: the retry launch redoes this node
             if (threadIdx.x == 0) retry[atomicAdd(d_retry, 1u)] = u;
         } else {
-            rate_select(A, u, keys, sc, cm, cap, red, used, ndist);
+            rate_select<TC>(A, u, keys, sc, cm, cap, red, used, ndist);
         }
         if (gtab) {  // rate_select ends with a barrier: empty the listed slots
             for (u32 t = threadIdx.x; t < ndist; t += blockDim.x) {
@@ -525,8 +533,18 @@ __global__ void k_sum_max(const u64 *__restrict__ v, u32 n, unsigned long long *
 }
 
 void setup_coarsen_kernels(Ctx &c) {
-    AXC_CUDA(cudaFuncSetAttribute(k_rate_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 16384 * 4));
+    AXC_CUDA(cudaFuncSetAttribute(k_rate_block<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 16384 * 4));
+    AXC_CUDA(cudaFuncSetAttribute(k_rate_block<(int)AXC_MAX_CANDIDATES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  3 * 16384 * 4));
 }
+
+// A rating kernel with per-thread top lists of 4 when cnc <= 4 (the reference scripts' -cnc 4),
+// else of AXC_MAX_CANDIDATES: shorter lists hold fewer registers, so more blocks fit an SM.
+#define RATE_LAUNCH(c, kname, cnc, grid, block, smem, ...)                                                   \
+    do {                                                                                                     \
+        if ((cnc) <= 4) LAUNCH_AS(c, #kname, kname<4>, grid, block, smem, __VA_ARGS__);                      \
+        else LAUNCH_AS(c, #kname, kname<(int)AXC_MAX_CANDIDATES>, grid, block, smem, __VA_ARGS__);           \
+    } while (0)
 
 void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 cnc, u32 *pairs, u32 *scores,
             u64 *pin_visits) {
@@ -570,7 +588,7 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     }
     // tier: one warp per node, table in static smem
     u32 nl = (u32)h[0];
-    LAUNCH(c, k_rate_warp, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
+    RATE_LAUNCH(c, k_rate_warp, cnc, cdiv(nl, RT_WARPS), RT_WARPS * 32, 0, A, list, nl);
     // tier: one block per node, 4096-slot table in dynamic smem
     nl = (u32)h[1];
     // shared tables sized by the largest node table the tier can need (distinct neighbours never
@@ -592,22 +610,22 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     auto block_tier = [&](const u32 *lst, u32 cnt, u32 cap_full) {
         if (!cnt) return;
         if (cap_full <= RT_TRY) {
-            LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * cap_full * 4, A, lst, cnt, cap_full, (u32 *)nullptr,
+            RATE_LAUNCH(c, k_rate_block, cnc, cnt, RT_BLOCK, 3 * cap_full * 4, A, lst, cnt, cap_full, (u32 *)nullptr,
                    (const u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
             return;
         }
         AXC_CUDA(cudaMemsetAsync(d_retry, 0, 8, c.stream));  // d_retry and d_retry2
-        LAUNCH(c, k_rate_block, cnt, RT_BLOCK, 3 * RT_TRY * 4, A, lst, cnt, RT_TRY, (u32 *)nullptr,
+        RATE_LAUNCH(c, k_rate_block, cnc, cnt, RT_BLOCK, 3 * RT_TRY * 4, A, lst, cnt, RT_TRY, (u32 *)nullptr,
                (const u32 *)nullptr, retry, d_retry, (u32 *)nullptr);
         const u32 *rl = retry, *dn = d_retry;
         if (cap_full > RT_MID) {
-            LAUNCH(c, k_rate_block, std::min<u32>(cnt, (u32)c.sms * 2), RT_BLOCK, 3 * RT_MID * 4, A, rl, cnt, RT_MID,
+            RATE_LAUNCH(c, k_rate_block, cnc, std::min<u32>(cnt, (u32)c.sms * 2), RT_BLOCK, 3 * RT_MID * 4, A, rl, cnt, RT_MID,
                    (u32 *)nullptr, dn, retry2, d_retry2, (u32 *)nullptr);
             rl = retry2;
             dn = d_retry2;
         }
         const u32 grid = std::min<u32>(cnt, (u32)c.sms * 2);
-        LAUNCH(c, k_rate_block, grid, RT_BLOCK, 3 * cap_full * 4, A, rl, cnt, cap_full, (u32 *)nullptr, dn,
+        RATE_LAUNCH(c, k_rate_block, cnc, grid, RT_BLOCK, 3 * cap_full * 4, A, rl, cnt, cap_full, (u32 *)nullptr, dn,
                (u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
     };
     block_tier(list2, nl, cap1);
@@ -629,12 +647,12 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
             AXC_CUDA(cudaMemsetAsync(gtab, 0xFF, (size_t)nl * cap * 4, c.stream));
             AXC_CUDA(cudaMemsetAsync(gtab + (u64)nl * cap, 0, (size_t)nl * cap * 8, c.stream));
             LAUNCH(c, k_rate_split_acc, nl * splits, RT_BLOCK, 0, A, list4, nl, cap, splits, gtab);
-            LAUNCH(c, k_rate_split_select, nl, RT_BLOCK, 0, A, list4, nl, cap, gtab);
+            RATE_LAUNCH(c, k_rate_split_select, cnc, nl, RT_BLOCK, 0, A, list4, nl, cap, gtab);
         } else {
             u32 grid = nl < (u32)c.sms * 2 ? nl : (u32)c.sms * 2;
             u32 *gtab = c.arena.alloc<u32>((u64)grid * 3 * cap), *gused = c.arena.alloc<u32>((u64)grid * cap);
             if (c.profiling("k_rate_block")) c.prof_bytes += 4 * tier_visits[2] + 8ull * cnc * nl;
-            LAUNCH(c, k_rate_block, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab, (const u32 *)nullptr, (u32 *)nullptr,
+            RATE_LAUNCH(c, k_rate_block, cnc, grid, RT_BLOCK, 0, A, list4, nl, cap, gtab, (const u32 *)nullptr, (u32 *)nullptr,
                    (u32 *)nullptr, gused);
         }
     }

@@ -141,6 +141,25 @@ struct Ctx {
         }                                                                                      \
     } while (0)
 
+// The same with the kernel timer's name given: for template instances of one kernel, which the
+// timer knows by the template's name.
+#define LAUNCH_AS(ctx, name, kern, grid, block, smem, ...)                                     \
+    do {                                                                                       \
+        if ((grid) > 0) {                                                                      \
+            const bool _prof = (ctx).profiling(name);                                          \
+            cudaEvent_t _e0 = _prof ? (ctx).prof_event() : nullptr;                           \
+            if (_e0) (ctx).prof_record(_e0);                                                   \
+            kern<<<(grid), (block), (smem), (ctx).stream>>>(__VA_ARGS__);                      \
+            (ctx).launches++;                                                                  \
+            AXC_CUDA(cudaGetLastError());                                                      \
+            if (_e0) {                                                                         \
+                cudaEvent_t _e1 = (ctx).prof_event();                                          \
+                if (_e1) (ctx).prof_record(_e1);                                               \
+                else (ctx).prof_used--;                                                        \
+            }                                                                                  \
+        }                                                                                      \
+    } while (0)
+
 inline u32 cdiv(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
 
 // Read `count` u64 scalars back from device memory (one small synchronous round trip).

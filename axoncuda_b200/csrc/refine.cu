@@ -2130,6 +2130,11 @@ struct LevelPrep {
 // environment variable AXC_CASCADE_BLOCK_MOVERS asks for it (a power of two >= 128), which sends
 // hyperedges with more movers to the scratch kernel; the tests use it to reach that kernel on
 // small inputs. Read at each level's launch, so it applies to the next partition.
+static bool round_loop_enabled() {
+    const char *s = std::getenv("AXC_ROUND_LOOP");
+    return !(s && s[0] == '0');
+}
+
 static u32 cascade_block_movers() {
     const char *s = std::getenv("AXC_CASCADE_BLOCK_MOVERS");
     if (!s || !*s) return CB_MOV_MAX;
@@ -2821,8 +2826,10 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
     const bool graph = R > 1;
     // Without the kernel timer the rounds run as one conditional WHILE graph: the schedule lives
     // on the device and the host waits once per level. With the timer on, each round is one replay
-    // of the round graph, so that its event pairs are read after every round.
-    if (graph && !c.prof_on) {
+    // of the round graph, so that its event pairs are read after every round. The environment
+    // variable AXC_ROUND_LOOP=0 also selects the replays (the same kernels and results; profilers
+    // that do not follow kernels into conditional graph nodes see them then).
+    if (graph && !c.prof_on && round_loop_enabled()) {
         const u32 done = refine_level_loop(c, L, lp, wfx, rp, part);
         c.arena.release(m);
         return done;
