@@ -109,7 +109,7 @@ typedef struct {
  * least connectivity is kept. With fewer than 2 copies the BFS chunks are refined alone. */
 #define AXC_KWAY_TRIES 16u
 #define AXC_KWAY_TRY_ROUNDS 32u
-#define AXC_KWAY_TRY_PINS 16777216ull
+#define AXC_KWAY_TRY_PINS 8388608ull
 
 typedef struct {
     uint32_t num_parts;        /* K' after zero-basing */
