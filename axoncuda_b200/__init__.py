@@ -81,7 +81,7 @@ EXPORTS = [
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
     "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
-    "axc_serve_configure", "axc_selftest_bounded_wait",
+    "axc_serve_configure", "axc_selftest_bounded_wait", "axc_tune_set",
 ]
 
 _lib = None
@@ -138,6 +138,8 @@ def lib() -> C.CDLL:
                                                      C.c_void_p, C.POINTER(C.c_int64)])
         sig["axc_serve_configure"] = (C.c_int, [C.c_void_p, C.c_uint32, C.c_size_t])
         sig["axc_partition_batch"] = (C.c_int, [C.c_void_p, C.c_uint32, H, P, C.POINTER(u32p), S])
+        sig["axc_tune_set"] = (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint64])
+        sig["axc_selftest_bounded_wait"] = (C.c_int, [C.c_void_p, C.c_uint32])
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res
@@ -336,6 +338,10 @@ class Context:
         st = Stats()
         self._check(lib().axc_poll(self._h, jid, _ptr(out, C.c_uint32), C.byref(st), timeout_ms), "axc_poll")
         return out[:n], st
+
+    def tune(self, key: str, value: int):
+        """axc_tune_set: a tile or table size, or an executor setting (see include/axc.h)."""
+        self._check(lib().axc_tune_set(self._h, key.encode(), C.c_uint64(value)), "axc_tune_set " + key)
 
     def serve_configure(self, lanes: int, device_budget: int = 0):
         """Lanes and device-memory budget of the batching / serving executor (before any submit)."""

@@ -36,6 +36,14 @@ Lane *lane_create(int device, int *rc);
 void lane_destroy(Lane *l);
 int lane_partition(Lane *l, size_t arena_bytes, const axc_hgraph *g, const axc_params *p, uint32_t *out_part,
                    axc_stats *stats, std::string *err);
+// tile and table sizes the lane's next jobs use (axc_tune_set's rate.try_slots, rate.mid_slots,
+// cascade.block_movers)
+void lane_tune(Lane *l, uint32_t rate_try, uint32_t rate_mid, uint32_t cascade_movers);
+// the context's own values of the same three, their setter (AXC_ENOTFOUND for another key), and
+// the range check of the power-of-two sizes
+void ctx_tune_get(axc_ctx *ctx, uint32_t out[3]);
+int ctx_tune_set(axc_ctx *ctx, const std::string &key, uint64_t value);
+bool tune_pow2_in(uint64_t v, uint64_t lo, uint64_t hi);
 
 // splitmix64: seeds independent xoshiro streams per (seed, index) so generators are
 // deterministic under any thread count.

@@ -49,8 +49,28 @@ static size_t estimate_bytes(const axc_hgraph *g) {
     return (size_t)b;
 }
 
+// Tile and table sizes for the jobs of one size class: jobs of at least min_pins pins (the largest
+// such class applies; a job below every class uses the context's own values).
+struct TuneClass {
+    bool set = false;
+    uint64_t min_pins = 0;
+    uint32_t rate_try = 2048, rate_mid = 8192, cascade_movers = 0;
+};
+constexpr int TUNE_CLASSES = 8;
+
+// The executor's settings, given before the first submit (axc_serve_configure, axc_tune_set).
+struct ServeConfig {
+    uint32_t lanes = 1;
+    size_t budget = 0;
+    bool excl_set = false;
+    uint64_t excl_pins = 1000000;
+    TuneClass cls[TUNE_CLASSES];
+};
+
 struct Executor {
     int device = 0;
+    uint32_t defaults[3] = {2048, 8192, 0};
+    TuneClass cls[TUNE_CLASSES];
     uint32_t nlanes = 1;
     size_t budget = 0;
     std::vector<Lane *> lanes;
@@ -102,6 +122,13 @@ struct Executor {
                 ++running;
             }
             j->t_start = Clock::now();
+            {  // the job's size class picks the lane's tile and table sizes
+                const TuneClass *best = nullptr;
+                for (const TuneClass &t : cls)
+                    if (t.set && j->pins >= t.min_pins && (!best || t.min_pins > best->min_pins)) best = &t;
+                if (best) lane_tune(lane, best->rate_try, best->rate_mid, best->cascade_movers);
+                else lane_tune(lane, defaults[0], defaults[1], defaults[2]);
+            }
             std::string err;
             const int rc = lane_partition(lane, j->est, &j->view, &j->p, j->part.data(), &j->st, &err);
             j->t_end = Clock::now();
@@ -175,7 +202,7 @@ struct Executor {
 // by shared_ptr so that a poller waiting on it keeps it alive while the context shuts down
 static std::mutex g_mu;
 static std::map<axc_ctx *, std::shared_ptr<Executor>> g_exec;
-static std::map<axc_ctx *, std::pair<uint32_t, size_t>> g_config;
+static std::map<axc_ctx *, ServeConfig> g_config;
 
 static std::shared_ptr<Executor> executor_for(axc_ctx *ctx, int *rc) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -185,12 +212,17 @@ static std::shared_ptr<Executor> executor_for(axc_ctx *ctx, int *rc) {
         return it->second;
     }
     auto x = std::make_shared<Executor>();
-    auto cfg = g_config.find(ctx);
-    x->nlanes = cfg != g_config.end() ? cfg->second.first : 1;
-    size_t budget = cfg != g_config.end() ? cfg->second.second : 0;
+    ServeConfig cfg;
+    if (auto it2 = g_config.find(ctx); it2 != g_config.end()) cfg = it2->second;
+    x->nlanes = cfg.lanes;
+    size_t budget = cfg.budget;
     if (budget == 0) budget = device_free_bytes(ctx_device(ctx)) / 2;
     x->budget = budget;
-    if (const char *e = std::getenv("AXC_SERVE_EXCLUSIVE_PINS")) x->excl_pins = std::strtoull(e, nullptr, 10);
+    x->excl_pins = cfg.excl_pins;
+    if (const char *e = std::getenv("AXC_SERVE_EXCLUSIVE_PINS"); e && !cfg.excl_set)
+        x->excl_pins = std::strtoull(e, nullptr, 10);
+    for (int i = 0; i < TUNE_CLASSES; ++i) x->cls[i] = cfg.cls[i];
+    ctx_tune_get(ctx, x->defaults);
     *rc = x->start(ctx_device(ctx));
     if (*rc) return nullptr;
     g_exec[ctx] = x;
@@ -218,7 +250,46 @@ extern "C" int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_b
     if (!ctx || lanes == 0 || lanes > 256) return AXC_EINVAL;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_exec.count(ctx)) return AXC_EBUSY;  // already serving
-    g_config[ctx] = {lanes, device_budget};
+    ServeConfig &cfg = g_config[ctx];
+    cfg.lanes = lanes;
+    cfg.budget = device_budget;
+    return AXC_OK;
+}
+
+extern "C" int axc_tune_set(axc_ctx *ctx, const char *key, uint64_t value) {
+    if (!ctx || !key) return AXC_EINVAL;
+    const std::string k(key);
+    if (k.rfind("serve.", 0) != 0 && k.rfind("class.", 0) != 0) return ctx_tune_set(ctx, k, value);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_exec.count(ctx)) return AXC_EBUSY;  // the executor has started
+    ServeConfig &cfg = g_config[ctx];
+    if (k == "serve.exclusive_pins") {
+        cfg.excl_pins = value;
+        cfg.excl_set = true;
+        return AXC_OK;
+    }
+    // class.<i>.<field>
+    const size_t dot = k.find('.', 6);
+    if (dot == std::string::npos || dot != 7) return AXC_ENOTFOUND;
+    const char ci = k[6];
+    if (ci < '0' || ci >= '0' + TUNE_CLASSES) return AXC_ENOTFOUND;
+    TuneClass &t = cfg.cls[ci - '0'];
+    const std::string field = k.substr(dot + 1);
+    if (field == "min_pins") {
+        t.min_pins = value;
+    } else if (field == "rate.try_slots") {
+        if (!tune_pow2_in(value, 64, 16384)) return AXC_EINVAL;
+        t.rate_try = (uint32_t)value;
+    } else if (field == "rate.mid_slots") {
+        if (!tune_pow2_in(value, 64, 16384)) return AXC_EINVAL;
+        t.rate_mid = (uint32_t)value;
+    } else if (field == "cascade.block_movers") {
+        if (value != 0 && !tune_pow2_in(value, 128, 2048)) return AXC_EINVAL;
+        t.cascade_movers = (uint32_t)value;
+    } else {
+        return AXC_ENOTFOUND;
+    }
+    t.set = true;
     return AXC_OK;
 }
 

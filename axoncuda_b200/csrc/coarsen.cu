@@ -24,8 +24,8 @@ __host__ __device__ __forceinline__ u32 rated_len(u64 len) { return len <= AXC_R
 constexpr u32 RT_WARP_W = 256;     // work (incident pins) handled by one warp
 constexpr u32 RT_BLK1_W = 2048;    // block tier 1: table 4096 slots (48 KiB)
 constexpr u32 RT_BLK2_W = 8192;    // block tier 2: table 16384 slots (192 KiB)
-constexpr u32 RT_TRY = 2048;       // first-try table of the block tiers (24 KiB)
-constexpr u32 RT_MID = 8192;       // second try of the larger tier (96 KiB, two blocks per SM)
+// The block tiers' first-try table (c.tune.rate_try slots, 2048 by default: 24 KiB) and the
+// second try of the larger tier (c.tune.rate_mid, 8192: 96 KiB, two blocks per SM) are tunable.
 constexpr u32 RT_WARPS = 4;
 constexpr u32 RT_BLOCK = 256;
 
@@ -601,25 +601,26 @@ void rating(Ctx &c, const DLevel &L, const u32 *wfx, u32 omega, u32 delta, u32 c
     };
     const u32 cap1 = tier_cap(RT_BLK1_W, 4096u), cap2 = tier_cap(RT_BLK2_W, 16384u);
     // Nodes' work bounds count pins with multiplicity; their distinct neighbours are usually far
-    // fewer. A first launch tries RT_TRY-slot tables (more blocks per SM); nodes that outgrow
+    // fewer. A first launch tries rt_try-slot tables (more blocks per SM); nodes that outgrow
     // theirs are redone by a second launch with the tier's full tables.
-    // A node that outgrows an RT_TRY table retries at RT_MID slots (two blocks per SM) when the
+    // A node that outgrows an rt_try table retries at rt_mid slots (two blocks per SM) when the
     // tier's tables are larger still, and only past that at the tier's full size.
     u32 *retry = c.arena.alloc<u32>(n), *retry2 = c.arena.alloc<u32>(n);
     u32 *d_retry = (u32 *)(dc + 4), *d_retry2 = d_retry + 1;  // dc[4] was read already
+    const u32 rt_try = c.tune.rate_try, rt_mid = std::max(c.tune.rate_mid, c.tune.rate_try);
     auto block_tier = [&](const u32 *lst, u32 cnt, u32 cap_full) {
         if (!cnt) return;
-        if (cap_full <= RT_TRY) {
+        if (cap_full <= rt_try) {
             RATE_LAUNCH(c, k_rate_block, cnc, cnt, RT_BLOCK, 3 * cap_full * 4, A, lst, cnt, cap_full, (u32 *)nullptr,
                    (const u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr, (u32 *)nullptr);
             return;
         }
         AXC_CUDA(cudaMemsetAsync(d_retry, 0, 8, c.stream));  // d_retry and d_retry2
-        RATE_LAUNCH(c, k_rate_block, cnc, cnt, RT_BLOCK, 3 * RT_TRY * 4, A, lst, cnt, RT_TRY, (u32 *)nullptr,
+        RATE_LAUNCH(c, k_rate_block, cnc, cnt, RT_BLOCK, 3 * rt_try * 4, A, lst, cnt, rt_try, (u32 *)nullptr,
                (const u32 *)nullptr, retry, d_retry, (u32 *)nullptr);
         const u32 *rl = retry, *dn = d_retry;
-        if (cap_full > RT_MID) {
-            RATE_LAUNCH(c, k_rate_block, cnc, std::min<u32>(cnt, (u32)c.sms * 2), RT_BLOCK, 3 * RT_MID * 4, A, rl, cnt, RT_MID,
+        if (cap_full > rt_mid) {
+            RATE_LAUNCH(c, k_rate_block, cnc, std::min<u32>(cnt, (u32)c.sms * 2), RT_BLOCK, 3 * rt_mid * 4, A, rl, cnt, rt_mid,
                    (u32 *)nullptr, dn, retry2, d_retry2, (u32 *)nullptr);
             rl = retry2;
             dn = d_retry2;

@@ -72,8 +72,18 @@ struct Arena {
     void release(size_t m) { top = m; }
 };
 
+// Tile and table sizes that change speed but never results (axc_tune_set): the block rating's
+// first-try and second-try tables (slots, powers of two) and the movers the cascade's
+// shared-memory block kernel keeps (0: its default, or AXC_CASCADE_BLOCK_MOVERS).
+struct Tune {
+    u32 rate_try = 2048;
+    u32 rate_mid = 8192;
+    u32 cascade_movers = 0;
+};
+
 struct Ctx {
     int device = 0;
+    Tune tune;
     int sms = 148;
     size_t smem_optin = 0;
     cudaStream_t stream = nullptr;

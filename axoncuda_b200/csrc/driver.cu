@@ -586,6 +586,40 @@ Lane *lane_create(int device, int *rc) {
     return l;
 }
 
+void lane_tune(Lane *l, uint32_t rate_try, uint32_t rate_mid, uint32_t cascade_movers) {
+    l->c.tune.rate_try = rate_try;
+    l->c.tune.rate_mid = rate_mid;
+    l->c.tune.cascade_movers = cascade_movers;
+}
+
+void ctx_tune_get(axc_ctx *ctx, uint32_t out[3]) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    out[0] = ctx->c.tune.rate_try;
+    out[1] = ctx->c.tune.rate_mid;
+    out[2] = ctx->c.tune.cascade_movers;
+}
+
+bool tune_pow2_in(uint64_t v, uint64_t lo, uint64_t hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+// The context's own tile and table sizes (include/axc.h axc_tune_set); AXC_ENOTFOUND for other keys.
+int ctx_tune_set(axc_ctx *ctx, const std::string &key, uint64_t v) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Tune &t = ctx->c.tune;
+    if (key == "rate.try_slots") {
+        if (!tune_pow2_in(v, 64, 16384)) return AXC_EINVAL;
+        t.rate_try = (u32)v;
+    } else if (key == "rate.mid_slots") {
+        if (!tune_pow2_in(v, 64, 16384)) return AXC_EINVAL;
+        t.rate_mid = (u32)v;
+    } else if (key == "cascade.block_movers") {
+        if (v != 0 && !tune_pow2_in(v, 128, 2048)) return AXC_EINVAL;
+        t.cascade_movers = (u32)v;
+    } else {
+        return AXC_ENOTFOUND;
+    }
+    return AXC_OK;
+}
+
 // One job on the lane in a fresh arena of `arena_bytes`. AXC_ENOMEM when the arena cannot be had
 // or turns out too small.
 int lane_partition(Lane *l, size_t arena_bytes, const axc_hgraph *g, const axc_params *p, uint32_t *out_part,

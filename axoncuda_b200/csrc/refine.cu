@@ -2126,22 +2126,25 @@ struct LevelPrep {
                              // hblock holds the hyperedges above CD_WARP_LEN pins
 };
 
-// Movers the cascade's block kernel keeps in shared memory: CB_MOV_MAX, or less when the
-// environment variable AXC_CASCADE_BLOCK_MOVERS asks for it (a power of two >= 128), which sends
-// hyperedges with more movers to the scratch kernel; the tests use it to reach that kernel on
-// small inputs. Read at each level's launch, so it applies to the next partition.
-static bool round_loop_enabled() {
-    const char *s = std::getenv("AXC_ROUND_LOOP");
-    return !(s && s[0] == '0');
-}
-
-static u32 cascade_block_movers() {
-    const char *s = std::getenv("AXC_CASCADE_BLOCK_MOVERS");
-    if (!s || !*s) return CB_MOV_MAX;
-    const unsigned long v = std::strtoul(s, nullptr, 10);
+// Movers the cascade's block kernel keeps in shared memory: CB_MOV_MAX, or less when the context's
+// tuning (c.tune.cascade_movers) or the environment variable AXC_CASCADE_BLOCK_MOVERS asks for it
+// (a power of two >= 128), which sends hyperedges with more movers to the scratch kernel; the tests
+// use it to reach that kernel on small inputs. Read at each level's launch.
+static u32 cascade_block_movers(const Ctx &c) {
+    unsigned long v = c.tune.cascade_movers;
+    if (!v) {
+        const char *s = std::getenv("AXC_CASCADE_BLOCK_MOVERS");
+        if (!s || !*s) return CB_MOV_MAX;
+        v = std::strtoul(s, nullptr, 10);
+    }
     u32 lim = 128;
     while ((unsigned long)lim * 2 <= v && lim < CB_MOV_MAX) lim <<= 1;
     return lim;
+}
+
+static bool round_loop_enabled() {
+    const char *s = std::getenv("AXC_ROUND_LOOP");
+    return !(s && s[0] == '0');
 }
 
 void setup_refine_kernels(Ctx &c) {
@@ -2560,7 +2563,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
             LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
             // block kernel: shared memory sized by the level's largest hyperedge, all resident blocks
             u32 smov = 128;
-            while (smov < lp.max_len && smov < cascade_block_movers()) smov <<= 1;
+            while (smov < lp.max_len && smov < cascade_block_movers(c)) smov <<= 1;
             // hashed tables: sized for the level's largest hyperedge within the block's limit
             const u32 stab = direct ? std::max(2 * rp.K, 32u)  // tk: the sweep's 2K lane masks
                                     : (u32)std::min<u64>(cascade_cap(std::min<u64>(lp.max_len, rp.K),

@@ -572,6 +572,11 @@ def percentiles(xs):
             "mean_ms": float(xs.mean())}
 
 
+def tuning_table(args):
+    """The autotuner's table for the batch and serve modes, when there is one."""
+    return args.tune if args.tune != "none" and os.path.exists(args.tune) else None
+
+
 def run_batch(args) -> dict:
     """jobs/s of the batched workload through the executor's lanes (axc_partition_batch) against a
     one-at-a-time loop of axc_partition over the same jobs; both from host buffers to host results."""
@@ -588,9 +593,15 @@ def run_batch(args) -> dict:
         t0 = time.perf_counter()
         solo = [seq.partition(g, p)[0] for g, p in jobs]
         t_seq = barrier_max(world, time.perf_counter() - t0)
+    tuning = tuning_table(args)
     with ax.Context(local, 256 << 20) as srv:
-        srv.serve_configure(args.lanes, int(args.budget_gb * (1 << 30)))
-        srv.partition_batch(jobs[:args.lanes])  # warm-up: lanes, graphs of the first levels
+        lanes = args.lanes
+        if tuning:  # the autotuner's table: size classes, exclusive threshold, lane count
+            from axoncuda_b200 import tune as T
+            lanes = lanes or T.apply(srv, tuning)
+        lanes = lanes or 8
+        srv.serve_configure(lanes, int(args.budget_gb * (1 << 30)))
+        srv.partition_batch(jobs[:lanes])  # warm-up: lanes, graphs of the first levels
         with Clocks(local) as clk:
             barrier(world)
             t0 = time.perf_counter()
@@ -602,7 +613,8 @@ def run_batch(args) -> dict:
             "unit": "jobs/s", "n_gpus": world, "higher_is_better": True, "scaling": "strong", "dtype": "u32",
             "data": "synthetic (seeded generators)",
             "config": {"workload": f"batch-{len(all_jobs)}", "jobs": len(all_jobs), "pins": pins,
-                       "lanes_per_gpu": args.lanes, "budget_gb": args.budget_gb,
+                       "lanes_per_gpu": lanes, "budget_gb": args.budget_gb,
+                       "tuning": os.path.relpath(tuning, ROOT) if tuning else "defaults",
                        "parallelism": f"jobs sharded over {world} GPU(s), no collective"},
             "sequential": {"value": len(all_jobs) / t_seq, "unit": "jobs/s", "seconds": t_seq},
             "speedup_vs_sequential": t_seq / t_bat, "seconds": t_bat, "pins_per_s": pins / t_bat,
@@ -635,9 +647,15 @@ def run_serve(args) -> dict:
         t = max(t, a) + s
         seq_lat.append((t - a) * 1e3)
     seq_span = t - arrivals[0]
+    tuning = tuning_table(args)
     with ax.Context(0, 256 << 20) as srv:
-        srv.serve_configure(args.lanes, int(args.budget_gb * (1 << 30)))
-        srv.partition_batch(reqs[:args.lanes])  # warm-up
+        lanes = args.lanes
+        if tuning:
+            from axoncuda_b200 import tune as T
+            lanes = lanes or T.apply(srv, tuning)
+        lanes = lanes or 8
+        srv.serve_configure(lanes, int(args.budget_gb * (1 << 30)))
+        srv.partition_batch(reqs[:lanes])  # warm-up
         done = {}
         ids = []
         with Clocks(0) as clk:
@@ -657,7 +675,8 @@ def run_serve(args) -> dict:
             "config": {"workload": "serve-poisson", "requests": len(reqs), "pins": pins,
                        "pins_per_request": f"log-uniform in [1e4, {args.serve_max_pins:.0e}]",
                        "arrival_rate_per_s": rate, "load_vs_sequential_capacity": args.serve_load,
-                       "lanes": args.lanes, "budget_gb": args.budget_gb},
+                       "lanes": lanes, "budget_gb": args.budget_gb,
+                       "tuning": os.path.relpath(tuning, ROOT) if tuning else "defaults"},
             "latency": percentiles(lat), "seconds": span,
             "sequential": {"value": len(reqs) / seq_span, "unit": "jobs/s", "capacity_jobs_per_s": cap,
                            "latency": percentiles(seq_lat)},
@@ -679,7 +698,10 @@ def main():
                     help="seconds one reference partition may take before its arm reports unavailable")
     ap.add_argument("--mode", default="partition", choices=["partition", "batch", "serve"],
                     help="partition: one hypergraph per step (the headline); batch / serve: many jobs")
-    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--lanes", type=int, default=0, help="executor lanes (0: the tuning table's, else 8)")
+    ap.add_argument("--tune", default=os.path.join(ROOT, "axoncuda_b200", "tuned_b200.json"),
+                    help="the autotuner's table (python -m axoncuda_b200.tune) for the batch and serve modes, "
+                         "or 'none'")
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--batch-jobs", type=int, default=256)
     ap.add_argument("--serve-requests", type=int, default=120)

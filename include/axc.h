@@ -244,6 +244,22 @@ int axc_gen_circuit(uint32_t n, uint32_t e, uint32_t smin, uint32_t smax, double
  * half the free device memory at the first submit. */
 int axc_serve_configure(axc_ctx *ctx, uint32_t lanes, size_t device_budget);
 int axc_submit(axc_ctx *ctx, const axc_hgraph *g, const axc_params *p, uint64_t *job_id);
+/* Tile and table sizes and executor settings (no reference counterpart: the reference's are
+ * compile-time constants, headers/defines.cuh). None of them changes a result, only speed; the
+ * autotuner axoncuda_b200/tune.py picks them per job-size class. Keys:
+ *   rate.try_slots, rate.mid_slots  the block rating's first-try and second-try hash tables (slots, a
+ *                                   power of two in [64, 16384]; defaults 2048 and 8192)
+ *   cascade.block_movers            movers the cascade's shared-memory block kernel keeps (0 = its
+ *                                   default of 2048, else a power of two in [128, 2048])
+ *   serve.exclusive_pins            submitted jobs of at least this many pins run alone (0 = none;
+ *                                   default 1,000,000)
+ *   class.<i>.min_pins, class.<i>.rate.try_slots, class.<i>.rate.mid_slots,
+ *   class.<i>.cascade.block_movers  for submitted jobs: size class i (0..7) covers jobs of at least
+ *                                   min_pins pins (the largest such class applies) and sets their
+ *                                   sizes; jobs below every class use the context's own.
+ * The first three apply to the context's own calls at once; serve.* and class.* must come before
+ * the first submit (AXC_EBUSY after it). Unknown keys give AXC_ENOTFOUND, bad values AXC_EINVAL. */
+int axc_tune_set(axc_ctx *ctx, const char *key, uint64_t value);
 /* Wait up to timeout_ms (<0: forever) for a job; copies its partition into out_part[n]. A job
  * still queued when the context is destroyed is answered with AXC_ECANCELED. */
 int axc_poll(axc_ctx *ctx, uint64_t job_id, uint32_t *out_part, axc_stats *stats, int timeout_ms);

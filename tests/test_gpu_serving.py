@@ -106,3 +106,32 @@ def test_destroy_answers_waiting_pollers():
         assert not t.is_alive()
     assert all(rc in (0, 12) for rc in rcs.values()), rcs  # AXC_OK or AXC_ECANCELED
     assert 12 in rcs.values()  # the last jobs were still queued behind the running one
+
+
+def test_tuning_changes_speed_not_results(ctx):
+    """axc_tune_set: every tile and table size gives the same partitions; bad values and unknown
+    keys are refused; executor settings are refused once the executor has started."""
+    jobs = mixed_jobs(6, seed0=500)
+    solo = [ctx.partition(g, p)[0] for g, p in jobs]
+    with ax.Context(0, 1 << 30) as c2:
+        for key, value in (("rate.try_slots", 256), ("rate.mid_slots", 1024), ("cascade.block_movers", 128)):
+            c2.tune(key, value)
+        for (g, p), s in zip(jobs, solo):
+            np.testing.assert_array_equal(c2.partition(g, p)[0], s)
+        for key, value, code in (("rate.try_slots", 3000, 1), ("cascade.block_movers", 64, 1), ("no.such", 1, 8)):
+            with pytest.raises(ax.AxcError) as e:
+                c2.tune(key, value)
+            assert e.value.code == code
+    with ax.Context(0, 256 << 20) as srv:
+        srv.serve_configure(3, 8 << 30)
+        srv.tune("class.0.min_pins", 0)
+        srv.tune("class.0.rate.try_slots", 512)
+        srv.tune("class.1.min_pins", 50000)
+        srv.tune("class.1.cascade.block_movers", 256)
+        srv.tune("serve.exclusive_pins", 0)
+        res = srv.partition_batch(jobs)
+        for (part, st), s in zip(res, solo):
+            np.testing.assert_array_equal(part, s)
+        with pytest.raises(ax.AxcError) as e:
+            srv.tune("class.2.min_pins", 1)
+        assert e.value.code == 9  # AXC_EBUSY
