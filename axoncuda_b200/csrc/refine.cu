@@ -302,6 +302,7 @@ struct GainArgs {
     int encourage;
     const u64 *off;
     const u32 *lam, *cpart, *ccnt, *cdcnt, *wfx;
+    const u32 *pins, *nsrc;  // the level's hyperedges (pin-centric passes)
     const u64 *toff;
     const u32 *touch, *nin, *nsize, *part;
     const u64 *psize, *pinb;
@@ -848,25 +849,48 @@ __global__ void __launch_bounds__(GN_BLOCK) k_gain_block(GainArgs A0, const u32 
 //  - k_gain_sample (one block per node, the sample table in shared memory) finds the sample
 //    prefix, accumulates the sampled connectivity and, when the prefix is the whole node, settles
 //    the node exactly as k_gain_block would; otherwise it writes the node's candidates;
-//  - k_gain_cands (one block per node, no table) sums every incidence's census entries against
-//    those few candidates in registers and picks the best feasible one.
+//  - k_cands_warp / k_cands_block (one warp or block per hyperedge holding such a node) put the
+//    hyperedge's census in a hash table and add, for each such pin, the hyperedge's weight to its
+//    candidates' sums, and k_cands_best picks each node's best feasible candidate. A node's exact
+//    pass so costs its incidences times GS_C + 1 lookups, not its whole census.
 constexpr u32 GS_K = AXC_SPARSE_GAIN_K;
 constexpr u32 GS_SAMPLE = AXC_SPARSE_GAIN_SAMPLE;
 constexpr u32 GS_C = AXC_SPARSE_GAIN_CANDIDATES;
 constexpr u32 GS_TAB = 2 * GS_SAMPLE;                // sample table slots: at most half full
 constexpr u32 GS_BLOCK = 256;
-constexpr size_t GS_SMEM = (size_t)GS_TAB * 16;      // conn u64, keys u32, inbound u32 per slot
-constexpr u32 GS_DONE = 0xFFFFFFFEu;                 // cand[u*GS_C]: settled by the sample kernel
-constexpr u32 GS_TOMB = 0xFFFFFFFEu;                 // a sample-table key taken out of the selection
-constexpr u32 GS_CAND_BLOCK = 256;
-constexpr u32 GS_CAND_PER_SM = 4;                   // resident blocks of k_gain_cands per SM
+constexpr size_t GS_SMEM = (size_t)GS_TAB * 16 + (size_t)GS_SAMPLE * 4;  // conn u64, keys u32,
+                                                     // inbound u32 per slot; the used-slot list
 // Nodes outside the sampled kernels (gain tiers 0 and 1) have at most GN_BLOCK_W census entries,
 // so their sample would be the whole node and the exact kernels give the rule's result.
 static_assert(GN_BLOCK_W <= GS_SAMPLE, "tier-1 nodes must fit the sample");
 
+// The census entries [ao, ao + lo) of one hyperedge read by the whole calling warp, CF_UNROLL
+// independent loads in flight per lane: f(k, cpart[k], w, inbound) for each entry k.
+constexpr u32 CF_UNROLL = 8;
+template <class F>
+__device__ __forceinline__ void census_edge_warp(const GainArgs &A, u64 ao, u32 lo, u32 w, u32 io, F &&f) {
+    const u32 lane = threadIdx.x & 31u;
+    for (u32 i0 = 0; i0 < lo; i0 += 32 * CF_UNROLL) {
+        u32 x[CF_UNROLL];
+#pragma unroll
+        for (u32 r = 0; r < CF_UNROLL; ++r) {
+            const u32 i = i0 + 32 * r + lane;
+            x[r] = i < lo ? A.cpart[ao + i] : NONE;
+        }
+#pragma unroll
+        for (u32 r = 0; r < CF_UNROLL; ++r) {
+            const u32 i = i0 + 32 * r + lane;
+            if (i < lo) f(ao + i, x[r], w, io);
+        }
+    }
+}
+
 // Census entries of u's incidences j = first, first + stride, ... below jend, flattened across the
-// calling warp's lanes in batches of 32 incidences (the scheme of gain_flat): f(k, w, inbound) is
-// called for each entry k, and every incidence adds its weight to wtot once (per lane).
+// calling warp's lanes in batches of 32 incidences (the scheme of gain_flat): f(k, cpart[k], w,
+// inbound) is called for each entry k, and every incidence adds its weight to wtot once (per
+// lane). A batch whose entries average CF_LONG or more per incidence is read one hyperedge at a
+// time by the whole warp instead (coalesced, no search). The calls are the same set either way.
+constexpr u32 CF_LONG = 16;
 template <class F>
 __device__ __forceinline__ void census_flat(const GainArgs &A, u32 u, u32 first, u32 stride, u32 jend, i64 &wtot,
                                             F &&f) {
@@ -890,6 +914,15 @@ __device__ __forceinline__ void census_flat(const GainArgs &A, u32 u, u32 first,
         }
         const u32 total = __shfl_sync(0xFFFFFFFFu, x, 31), excl = x - lm;
         const u32 chunk = (jend - jb) < 32 ? (jend - jb) : 32;
+        if (total >= 32 * CF_LONG) {  // long lists: the warp reads one hyperedge's entries at a time
+            for (u32 t = 0; t < chunk; ++t) {
+                const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, t);
+                const u32 lo = __shfl_sync(0xFFFFFFFFu, lm, t), wo = __shfl_sync(0xFFFFFFFFu, wh, t);
+                const u32 io = __shfl_sync(0xFFFFFFFFu, ib, t);
+                census_edge_warp(A, ao, lo, wo, io, f);
+            }
+            continue;
+        }
         for (u32 fb = 0; fb < total; fb += 32) {
             const u32 fi = fb + lane;
             u32 lo = 0, hi = chunk - 1;
@@ -902,8 +935,25 @@ __device__ __forceinline__ void census_flat(const GainArgs &A, u32 u, u32 first,
             const u64 ao = __shfl_sync(0xFFFFFFFFu, ah, lo);
             const u32 wo = __shfl_sync(0xFFFFFFFFu, wh, lo);
             const u32 io = __shfl_sync(0xFFFFFFFFu, ib, lo);
-            if (fi < total) f(ao + (fi - eo), wo, io);
+            if (fi < total) f(ao + (fi - eo), A.cpart[ao + (fi - eo)], wo, io);
         }
+    }
+}
+
+// Census entries of u's incidences j = first, first + stride, ... below jend, one incidence per
+// warp at a time (the calling warp's `first` and `stride` are multiples of one incidence): for
+// nodes whose few incidences have long entry lists. Same calls as census_flat; lane 0 adds each
+// incidence's weight to wtot.
+template <class F>
+__device__ __forceinline__ void census_edges(const GainArgs &A, u32 u, u32 first, u32 stride, u32 jend, i64 &wtot,
+                                             F &&f) {
+    const u64 t0 = A.toff[u];
+    const u32 nin_u = A.nin[u];
+    for (u32 j = first; j < jend; j += stride) {
+        const u32 h = A.touch[t0 + j];
+        const u32 w = A.wfx[h];
+        if ((threadIdx.x & 31u) == 0) wtot += w;
+        census_edge_warp(A, A.off[h], A.lam[h], w, j < nin_u ? 1u : 0u, f);
     }
 }
 
@@ -927,24 +977,67 @@ __device__ __forceinline__ bool skey_better(const SKey &a, const SKey &b) {
     return a.hi > b.hi || (a.hi == b.hi && a.lo > b.lo);
 }
 
-__global__ void __launch_bounds__(GS_BLOCK) k_gain_sample(GainArgs A0, const u32 *__restrict__ list, u32 nl,
-                                                          u32 *__restrict__ cand) {
+// Candidates and accumulator rows of the sampled rule's exact pass (k_cands_*).
+struct CandAcc {
+    u32 *spos;                 // [n]
+    u32 *cand;                 // [n * GS_C], NONE-padded
+    unsigned long long *conn;  // [rows * GS_C]
+    u32 *dcon;                 // [rows * GS_C]
+    unsigned long long *sacc, *wacc;  // [rows]
+};
+
+// Inserts k into the descending list top[0, GS_C) (keys not above the last entry drop out).
+__device__ __forceinline__ void skey_insert(SKey (&top)[GS_C], SKey k) {
+#pragma unroll
+    for (u32 i = 0; i < GS_C; ++i)
+        if (skey_better(k, top[i])) {
+            const SKey t = top[i];
+            top[i] = k;
+            k = t;
+        }
+}
+// The warp's best of its lanes' lists, GS_C times: out[r] = the r-th best over the warp (empty
+// keys are {0, 0}, below every real key, whose low word holds ~q with q < 2^32 - 2).
+__device__ __forceinline__ void skey_warp_top(SKey (&top)[GS_C], SKey *out) {
+    const u32 lane = threadIdx.x & 31u;
+    for (u32 r = 0; r < GS_C; ++r) {
+        SKey b = top[0];
+        u32 bl = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const SKey c{__shfl_xor_sync(0xFFFFFFFFu, b.hi, o), __shfl_xor_sync(0xFFFFFFFFu, b.lo, o)};
+            const u32 cl = __shfl_xor_sync(0xFFFFFFFFu, bl, o);
+            if (skey_better(c, b) || (!skey_better(b, c) && cl < bl)) { b = c; bl = cl; }
+        }
+        if (lane == 0) out[r] = b;
+        if (lane == bl) {  // the winner drops its head
+#pragma unroll
+            for (u32 i = 0; i + 1 < GS_C; ++i) top[i] = top[i + 1];
+            top[GS_C - 1] = SKey{0, 0};
+        }
+    }
+}
+
+__global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+                                                             CandAcc C) {
     const GainArgs A = gain_args_now(A0);
     extern __shared__ unsigned long long gs_dyn[];
     unsigned long long *sconn = gs_dyn;      // [GS_TAB]
     u32 *keys = (u32 *)(gs_dyn + GS_TAB);    // [GS_TAB]
     u32 *sdc = keys + GS_TAB;                // [GS_TAB]
+    u32 *used = sdc + GS_TAB;                // [GS_SAMPLE]: the slots the node filled
     __shared__ unsigned long long wsh[GS_BLOCK / 32];
     __shared__ unsigned long long s_acc;
     __shared__ Cand cred[GS_BLOCK / 32];
-    __shared__ SKey kred[GS_BLOCK / 32];
-    __shared__ u32 sred[GS_BLOCK / 32];
+    __shared__ SKey kred[(GS_BLOCK / 32) * GS_C];
+    __shared__ u32 ndist;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sconn[i] = 0; sdc[i] = 0; }
     for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
         const u32 u = list[idx], p = A.part[u];
         const u64 t0 = A.toff[u];
         const u32 deg = (u32)(A.toff[u + 1] - t0), nin_u = A.nin[u];
-        for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sconn[i] = 0; sdc[i] = 0; }
+        if (threadIdx.x == 0) ndist = 0;
         // 1. the sample: the longest incidence prefix with at most GS_SAMPLE census entries
         u32 m = 0;
         u64 acc = 0;
@@ -969,22 +1062,28 @@ __global__ void __launch_bounds__(GS_BLOCK) k_gain_sample(GainArgs A0, const u32
         }
         // 2. sampled connectivity; saving and wtot are exact when the sample is the whole node
         i64 saving = 0, wtot = 0;
-        census_flat(A, u, 32 * warp, GS_BLOCK, m, wtot, [&](u64 k, u32 w, u32 io) {
-            const u32 q = A.cpart[k];
+        const auto entry = [&](u64 k, u32 q, u32 w, u32 io) {
             if (q == p) { saving += leave_gain(A.encourage, w, A.ccnt[k]); return; }
-            const u32 slot = hash_find_or_insert(keys, GS_TAB - 1, q);
+            bool fresh = false;
+            const u32 slot = hash_insert_fresh(keys, GS_TAB - 1, q, fresh);
             if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
+            if (fresh) used[atomicAdd(&ndist, 1u)] = slot;  // at most GS_SAMPLE distinct keys
             atomicAdd(&sconn[slot], (unsigned long long)w);
             if (io && A.cdcnt[k] > 0) atomicAdd(&sdc[slot], 1u);
-        });
+        };
+        if (acc >= (u64)CF_LONG * m)  // few long incidences: one per warp, not 32 per warp
+            census_edges(A, u, warp, GS_BLOCK / 32, m, wtot, entry);
+        else
+            census_flat(A, u, 32 * warp, GS_BLOCK, m, wtot, entry);
         __syncthreads();
+        const u32 nd = ndist;
         const u64 s = A.nsize[u];
         if (m == deg) {  // 3a. the whole node: exact, as the table kernels
             saving = (i64)block_sum_u64((u64)saving, wsh);
             wtot = (i64)block_sum_u64((u64)wtot, wsh);
             Cand best{INT64_MIN, 0};
-            for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
-                if (keys[i] == NONE) continue;
+            for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {
+                const u32 i = used[t];
                 const Cand c = gain_candidate(A, u, keys[i], sconn[i], sdc[i], saving, wtot);
                 if (cand_better(c, best)) best = c;
             }
@@ -995,108 +1094,183 @@ __global__ void __launch_bounds__(GS_BLOCK) k_gain_sample(GainArgs A0, const u32
                 Cand b = cred[0];
                 for (u32 i = 1; i < GS_BLOCK / 32; ++i)
                     if (cand_better(cred[i], b)) b = cred[i];
-                write_move(A, u, b);
-                cand[(u64)u * GS_C] = GS_DONE;
+                write_move(A, u, b);  // spos[u] stays NONE
             }
+        } else {
+            // 3b. the GS_C best by (sampled connectivity, tie hash, -id) among the keys the size
+            // limit and the inbound bound do not rule out: per-thread lists, then per warp, then
+            // warp 0 over the warps' lists
+            const u64 in_sample = m < nin_u ? m : nin_u;
+            SKey top[GS_C];
+#pragma unroll
+            for (u32 r = 0; r < GS_C; ++r) top[r] = SKey{0, 0};
+            for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {
+                const u32 i = used[t], q = keys[i];
+                if (A.psize[q] + s - s / A.discount > A.omega || A.pinb[q] + in_sample - sdc[i] > A.delta) continue;
+                skey_insert(top, SKey{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
+            }
+            skey_warp_top(top, kred + warp * GS_C);
             __syncthreads();
-            continue;
-        }
-        // 3b. rule out what the size limit or the inbound bound excludes
-        const u64 in_sample = m < nin_u ? m : nin_u;
-        for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
-            const u32 q = keys[i];
-            if (q == NONE) continue;
-            if (A.psize[q] + s - s / A.discount > A.omega || A.pinb[q] + in_sample - sdc[i] > A.delta) keys[i] = GS_TOMB;
+            if (warp == 0) {
+#pragma unroll
+                for (u32 r = 0; r < GS_C; ++r) top[r] = SKey{0, 0};
+                for (u32 t = lane; t < (GS_BLOCK / 32) * GS_C; t += 32) skey_insert(top, kred[t]);
+                __syncwarp();  // every lane has read kred before lane 0 overwrites its head
+                skey_warp_top(top, kred);
+                __syncwarp();
+                if (lane < GS_C) {  // the candidates and a zeroed accumulator row (row = list index)
+                    const SKey b = kred[lane];
+                    C.cand[(u64)u * GS_C + lane] = (b.hi | b.lo) ? ~(u32)b.lo : NONE;
+                    C.conn[(u64)idx * GS_C + lane] = 0;
+                    C.dcon[(u64)idx * GS_C + lane] = 0;
+                }
+                if (lane == 0) {
+                    C.sacc[idx] = 0;
+                    C.wacc[idx] = 0;
+                    C.spos[u] = idx;
+                }
+            }
         }
         __syncthreads();
-        // 4. the GS_C best by (sampled connectivity, tie hash, -id), one block-wide maximum each
-        for (u32 r = 0; r < GS_C; ++r) {
-            SKey best{0, 0};
-            u32 bslot = NONE;
-            for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) {
-                const u32 q = keys[i];
-                if (q >= GS_TOMB) continue;
-                const SKey k{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)};
-                if (bslot == NONE || skey_better(k, best)) { best = k; bslot = i; }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                SKey o2{__shfl_xor_sync(0xFFFFFFFFu, best.hi, o), __shfl_xor_sync(0xFFFFFFFFu, best.lo, o)};
-                const u32 os = __shfl_xor_sync(0xFFFFFFFFu, bslot, o);
-                if (os != NONE && (bslot == NONE || skey_better(o2, best))) { best = o2; bslot = os; }
-            }
-            if (lane == 0) { kred[warp] = best; sred[warp] = bslot; }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                SKey b = kred[0];
-                u32 bs = sred[0];
-                for (u32 i = 1; i < GS_BLOCK / 32; ++i)
-                    if (sred[i] != NONE && (bs == NONE || skey_better(kred[i], b))) { b = kred[i]; bs = sred[i]; }
-                cand[(u64)u * GS_C + r] = bs == NONE ? NONE : keys[bs];
-                if (bs != NONE) keys[bs] = GS_TOMB;
-            }
-            __syncthreads();
+        for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {  // empty the node's slots for the next one
+            const u32 i = used[t];
+            keys[i] = NONE;
+            sconn[i] = 0;
+            sdc[i] = 0;
         }
+        __syncthreads();
     }
 }
 
-// The exact pass of the sampled rule: one block per listed node whose sample was not the whole
-// node; its candidates' connectivity and shared inbound counts over all incidences, then the best
-// feasible candidate (the order of gain_candidate).
-__global__ void __launch_bounds__(GS_CAND_BLOCK, GS_CAND_PER_SM) k_gain_cands(GainArgs A0, const u32 *__restrict__ list, u32 nl,
-                                                              const u32 *__restrict__ cand) {
-    const GainArgs A = gain_args_now(A0);
-    __shared__ unsigned long long wsh[GS_CAND_BLOCK / 32];
-    __shared__ unsigned long long csum[GS_CAND_BLOCK / 32][GS_C];
-    __shared__ u32 dsum[GS_CAND_BLOCK / 32][GS_C];
-    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
-        const u32 u = list[idx];
-        if (cand[(u64)u * GS_C] == GS_DONE) continue;  // uniform over the block
-        const u32 p = A.part[u];
-        const u32 deg = (u32)(A.toff[u + 1] - A.toff[u]);
-        u32 q[GS_C];
-        unsigned long long cc[GS_C];
-        u32 cd[GS_C];
-#pragma unroll
-        for (u32 i = 0; i < GS_C; ++i) {
-            const u32 v = cand[(u64)u * GS_C + i];
-            q[i] = v == NONE ? GS_TOMB : v;  // never equal to a partition id
-            cc[i] = 0;
-            cd[i] = 0;
-        }
-        i64 saving = 0, wtot = 0;
-        census_flat(A, u, 32 * warp, GS_CAND_BLOCK, deg, wtot, [&](u64 k, u32 w, u32 io) {
-            const u32 x = A.cpart[k];
-            if (x == p) { saving += leave_gain(A.encourage, w, A.ccnt[k]); return; }
-            const u32 dd = (io && A.cdcnt[k] > 0) ? 1u : 0u;
-#pragma unroll
-            for (u32 i = 0; i < GS_C; ++i)
-                if (x == q[i]) { cc[i] += w; cd[i] += dd; }
-        });
-        saving = (i64)block_sum_u64((u64)saving, wsh);
-        wtot = (i64)block_sum_u64((u64)wtot, wsh);
-#pragma unroll
-        for (u32 i = 0; i < GS_C; ++i) {
-            const u64 a = warp_sum((u64)cc[i]);
-            const u32 b = warp_sum(cd[i]);
-            if (lane == 0) { csum[warp][i] = a; dsum[warp][i] = b; }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            Cand best{INT64_MIN, 0};
-            for (u32 i = 0; i < GS_C; ++i) {
-                if (q[i] == GS_TOMB) continue;
-                u64 a = 0;
-                u32 b = 0;
-                for (u32 w2 = 0; w2 < GS_CAND_BLOCK / 32; ++w2) { a += csum[w2][i]; b += dsum[w2][i]; }
-                const Cand c = gain_candidate(A, u, q[i], a, b, saving, wtot);
-                if (cand_better(c, best)) best = c;
-            }
-            write_move(A, u, best);
-        }
-        __syncthreads();
+// The exact pass of the sampled rule, pin-centric. Each listed node u whose sample was not the
+// whole node has row r = spos[u] of the accumulators (k_gain_sample sets it and zeroes the row;
+// spos is NONE for every other node): conn[r * GS_C + i], the weight of u's hyperedges holding its
+// candidate i; dcon[r * GS_C + i], u's inbound hyperedges with a destination pin in candidate i;
+// sacc[r], u's saving from leaving its partition; wacc[r], the weight of all u's hyperedges. One
+// pass over the hyperedges fills them: a hyperedge's census goes into a hash table (partition ->
+// count, plus a has-destination bit) and each listed pin looks up its own partition and its
+// candidates. k_cands_best then takes the best feasible candidate from these integer sums, which
+// are those a scan of each node's incidences would give.
+static_assert(GS_C == 8, "k_cands_* read a node's candidates as two 16-byte words");
+constexpr u32 CV_DBIT = 0x80000000u;  // census value: the partition holds a destination pin
+constexpr u32 CV_WARPS = 4;
+constexpr u32 CV_WARP_LEN = 256;      // longer hyperedges take a block (CS_WARP_CAP)
+constexpr u32 CV_BLOCK_LEN = 4096;    // longer still: a table in device memory (CS_BLOCK_CAP)
+constexpr u32 CV_BLOCK = 256;
+constexpr size_t CV_BLOCK_SMEM = (size_t)2 * CV_BLOCK_LEN * 8;  // keys and values, 2 slots per pin
+
+// Census entries [a, a + lm) of one hyperedge into keys/vals (mask + 1 cleared slots), threads
+// t, t + nt, ...: each partition appears once in a census, so each slot is written once.
+__device__ __forceinline__ void cv_fill(const GainArgs &A, u64 a, u32 lm, u32 *keys, u32 *vals, u32 mask, u32 t,
+                                        u32 nt) {
+    for (u32 j = t; j < lm; j += nt) {
+        const u32 slot = hash_find_or_insert(keys, mask, A.cpart[a + j]);
+        if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); continue; }
+        vals[slot] = A.ccnt[a + j] | (A.cdcnt[a + j] > 0 ? CV_DBIT : 0u);
     }
+}
+// Listed pin v (row r) of a hyperedge of weight w; io: v is one of its destinations.
+__device__ __forceinline__ void cv_pin(const GainArgs &A, const CandAcc &C, u32 v, u32 r, bool io, u32 w,
+                                       const u32 *keys, const u32 *vals, u32 mask) {
+    const u32 sp = hash_find(keys, mask, A.part[v]);  // present: v's own partition
+    if (sp != NONE) {
+        const i64 g = leave_gain(A.encourage, w, vals[sp] & ~CV_DBIT);
+        if (g) atomicAdd(&C.sacc[r], (unsigned long long)g);
+    }
+    if (w) atomicAdd(&C.wacc[r], (unsigned long long)w);
+    const uint4 *cp = reinterpret_cast<const uint4 *>(C.cand + (u64)v * GS_C);
+    const uint4 c0 = cp[0], c1 = cp[1];
+    const u32 q[GS_C] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+    for (u32 i = 0; i < GS_C; ++i) {
+        if (q[i] == NONE) break;
+        const u32 s = hash_find(keys, mask, q[i]);
+        if (s == NONE) continue;
+        if (w) atomicAdd(&C.conn[(u64)r * GS_C + i], (unsigned long long)w);
+        if (io && (vals[s] & CV_DBIT)) atomicAdd(&C.dcon[(u64)r * GS_C + i], 1u);
+    }
+}
+
+// One warp per hyperedge of at most CV_WARP_LEN pins; skipped when it holds no listed pin.
+__global__ void __launch_bounds__(CV_WARPS * 32) k_cands_warp(GainArgs A, CandAcc C, u32 e) {
+    __shared__ u32 tk[CV_WARPS][2 * CV_WARP_LEN], tv[CV_WARPS][2 * CV_WARP_LEN];
+    const u32 wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 h = blockIdx.x * CV_WARPS + wp;
+    if (h >= e) return;
+    const u64 a = A.off[h], b = A.off[h + 1];
+    if (b - a > CV_WARP_LEN) return;
+    constexpr u32 R = CV_WARP_LEN / 32;
+    u32 pv[R], pr[R];
+    bool any = false;
+#pragma unroll
+    for (u32 i = 0; i < R; ++i) {
+        const u64 k = a + lane + 32 * i;
+        pv[i] = k < b ? A.pins[k] : 0;
+        pr[i] = k < b ? C.spos[pv[i]] : NONE;
+        any |= pr[i] != NONE;
+    }
+    if (!__any_sync(0xFFFFFFFFu, any)) return;
+    const u32 lm = A.lam[h];
+    u32 cap = 32;
+    while (cap < 2 * lm) cap <<= 1;
+    u32 *keys = tk[wp], *vals = tv[wp];
+    for (u32 i = lane; i < cap; i += 32) keys[i] = NONE;
+    __syncwarp();
+    cv_fill(A, a, lm, keys, vals, cap - 1, lane, 32);
+    __syncwarp();
+    const u32 w = A.wfx[h];
+    const u64 s = a + A.nsrc[h];
+#pragma unroll
+    for (u32 i = 0; i < R; ++i)
+        if (pr[i] != NONE) cv_pin(A, C, pv[i], pr[i], a + lane + 32 * i >= s, w, keys, vals, cap - 1);
+}
+
+// One block per listed hyperedge: `list` holds those of CV_WARP_LEN < |e| <= CV_BLOCK_LEN pins
+// (tables in shared memory) or, with gtab set, the longer ones (tables at gtab + 2 * gtab_off[i],
+// 2 * |e| slots rounded up to a power of two, as k_tab_sizes sizes them).
+__global__ void __launch_bounds__(CV_BLOCK) k_cands_block(GainArgs A, CandAcc C, const u32 *__restrict__ list,
+                                                          u32 nlist, u32 *gtab, const u64 *__restrict__ gtab_off) {
+    extern __shared__ u32 cv_dyn[];
+    if (blockIdx.x >= nlist) return;
+    const u32 h = list[blockIdx.x];
+    const u64 a = A.off[h], b = A.off[h + 1];
+    bool any = false;
+    for (u64 k = a + threadIdx.x; k < b && !any; k += CV_BLOCK) any = C.spos[A.pins[k]] != NONE;
+    if (!__syncthreads_or(any)) return;
+    const u32 lm = A.lam[h];
+    u32 cap = 32;
+    while (cap < 2 * lm) cap <<= 1;
+    u32 *keys = gtab ? gtab + 2 * gtab_off[blockIdx.x] : cv_dyn;
+    u32 *vals = keys + cap;
+    for (u32 i = threadIdx.x; i < cap; i += CV_BLOCK) keys[i] = NONE;
+    __syncthreads();
+    cv_fill(A, a, lm, keys, vals, cap - 1, threadIdx.x, CV_BLOCK);
+    __syncthreads();
+    const u32 w = A.wfx[h];
+    const u64 s = a + A.nsrc[h];
+    for (u64 k = a + threadIdx.x; k < b; k += CV_BLOCK) {
+        const u32 v = A.pins[k], r = C.spos[v];
+        if (r != NONE) cv_pin(A, C, v, r, k >= s, w, keys, vals, cap - 1);
+    }
+}
+
+// Each listed node with a row: its best feasible candidate (the order of gain_candidate).
+__global__ void k_cands_best(GainArgs A0, CandAcc C, const u32 *__restrict__ list, u32 nl) {
+    const GainArgs A = gain_args_now(A0);
+    const u32 idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nl) return;
+    const u32 u = list[idx], r = C.spos[u];
+    if (r == NONE) return;  // settled by k_gain_sample
+    const i64 saving = (i64)C.sacc[r], wtot = (i64)C.wacc[r];
+    Cand best{INT64_MIN, 0};
+#pragma unroll
+    for (u32 i = 0; i < GS_C; ++i) {
+        const u32 q = C.cand[(u64)u * GS_C + i];
+        if (q == NONE) break;
+        const Cand c = gain_candidate(A, u, q, C.conn[(u64)r * GS_C + i], C.dcon[(u64)r * GS_C + i], saving, wtot);
+        if (cand_better(c, best)) best = c;
+    }
+    write_move(A, u, best);
 }
 
 __global__ void k_list_degree(const u32 *__restrict__ list, u32 nl, const u64 *__restrict__ toff,
@@ -2097,7 +2271,7 @@ GainArgs make_gain_args(const DLevel &L, const u32 *wfx, const RefineParams &rp,
     GainArgs A;
     A.n = L.n; A.omega = rp.omega; A.delta = rp.delta; A.discount = discount; A.round = round; A.K = rp.K;
     A.seed = (u32)rp.seed; A.encourage = rp.encourage ? 1 : 0;
-    A.off = L.off; A.lam = cs.lam; A.cpart = cs.part; A.ccnt = cs.cnt; A.cdcnt = cs.dcnt; A.wfx = wfx;
+    A.off = L.off; A.pins = L.pins; A.nsrc = L.nsrc; A.lam = cs.lam; A.cpart = cs.part; A.ccnt = cs.cnt; A.cdcnt = cs.dcnt; A.wfx = wfx;
     A.toff = L.toff; A.touch = L.touch; A.nin = L.nin; A.nsize = L.nsize; A.part = part;
     A.psize = psize; A.pinb = pinb; A.target = target; A.gain = gain; A.status = status;
     A.dyn = nullptr;
@@ -2152,6 +2326,7 @@ void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
     AXC_CUDA(cudaFuncSetAttribute(k_cascade_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_DYN_MAX));
     AXC_CUDA(cudaFuncSetAttribute(k_gain_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM));
+    AXC_CUDA(cudaFuncSetAttribute(k_cands_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CV_BLOCK_SMEM));
     AXC_CUDA(cudaFuncSetAttribute(k_rank_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RSS_SMEM));
 }
 
@@ -2329,11 +2504,25 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
     }
     if (lp.ncount[2] && A.K > GS_K) {  // the sampled rule (include/axc.h AXC_SPARSE_GAIN_*)
         size_t m = c.arena.mark();
-        u32 *cand = c.arena.alloc<u32>((u64)L.n * GS_C);
-        const u32 g1 = std::min<u32>(lp.ncount[2], (u32)c.sms);
-        const u32 g2 = std::min<u32>(lp.ncount[2], (u32)c.sms * GS_CAND_PER_SM);
-        LAUNCH(c, k_gain_sample, g1, GS_BLOCK, GS_SMEM, A, lp.ntier[2], lp.ncount[2], cand);
-        LAUNCH(c, k_gain_cands, g2, GS_CAND_BLOCK, 0, A, lp.ntier[2], lp.ncount[2], (const u32 *)cand);
+        const u32 rows = lp.ncount[2];
+        CandAcc C;
+        C.cand = c.arena.alloc<u32>((u64)L.n * GS_C);
+        C.spos = c.arena.alloc<u32>(L.n);
+        C.conn = c.arena.alloc<unsigned long long>((u64)rows * GS_C);
+        C.dcon = c.arena.alloc<u32>((u64)rows * GS_C);
+        C.sacc = c.arena.alloc<unsigned long long>(rows);
+        C.wacc = c.arena.alloc<unsigned long long>(rows);
+        fill_u32(c, C.spos, NONE, L.n);
+        LAUNCH(c, k_gain_sample, std::min<u32>(rows, (u32)c.sms), GS_BLOCK, GS_SMEM, A, lp.ntier[2], rows, C);
+        LAUNCH(c, k_cands_warp, cdiv(L.e, CV_WARPS), CV_WARPS * 32, 0, A, C, L.e);
+        if (lp.n_hblock)
+            LAUNCH(c, k_cands_block, lp.n_hblock, CV_BLOCK, CV_BLOCK_SMEM, A, C, lp.hblock, lp.n_hblock, (u32 *)nullptr,
+                   (const u64 *)nullptr);
+        if (lp.n_hhuge) {
+            u32 *gtab = c.arena.alloc<u32>(2 * lp.huge_tot);
+            LAUNCH(c, k_cands_block, lp.n_hhuge, CV_BLOCK, 0, A, C, lp.hhuge, lp.n_hhuge, gtab, (const u64 *)lp.huge_tab);
+        }
+        LAUNCH(c, k_cands_best, cdiv(rows, 256), 256, 0, A, C, lp.ntier[2], rows);
         c.arena.release(m);
     } else if (lp.ncount[2]) {
         size_t m = c.arena.mark();
