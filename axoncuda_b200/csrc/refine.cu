@@ -33,6 +33,20 @@ constexpr u32 CS_WARP_CAP = 256;
 constexpr u32 CS_BLOCK_CAP = 4096;
 constexpr u32 CS_WARPS = 4;
 
+// Slots of a block's census or candidate hash table for `len` keys: a power of two, at most 2/3
+// full. The hyperedge's entries and their order do not depend on it.
+__host__ __device__ __forceinline__ u32 cs_cap(u64 len) {
+    u32 cap = 32;
+    while (cap < len + (len >> 1)) cap <<= 1;
+    return cap;
+}
+// Bytes of dynamic shared memory this launch was given.
+__device__ __forceinline__ u32 dyn_smem_bytes() {
+    u32 b;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(b));
+    return b;
+}
+
 // What a node saves by leaving partition p of a hyperedge (weight w) where p holds c of its pins:
 // INCC (encourage) floor(w / c^2), k-way w when the node is the last pin in p.
 __device__ __forceinline__ i64 leave_gain(int encourage, u32 w, u32 c) {
@@ -116,8 +130,11 @@ __global__ void k_census_block(const u32 *__restrict__ list, u32 nlist, CensusAr
     const u32 h = list[blockIdx.x];
     const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
     const u32 len = (u32)(b - a);
-    u32 cap = 32;
-    while (cap < 2 * len) cap <<= 1;
+    const u32 cap = cs_cap(len);
+    if (!gtab && 16ull * cap > dyn_smem_bytes()) {  // launched with too small a table: refuse
+        if (threadIdx.x == 0) atomicExch(A.status, DEV_HASH_FULL);
+        return;
+    }
     u32 *keys = gtab ? gtab + 4 * gtab_off[blockIdx.x] : dyn;
     u32 *mn = keys + cap, *cnt = mn + cap, *dcnt = cnt + cap;
     for (u32 i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = NONE; mn[i] = NONE; cnt[i] = 0; dcnt[i] = 0; }
@@ -857,7 +874,7 @@ constexpr u32 GS_K = AXC_SPARSE_GAIN_K;
 constexpr u32 GS_SAMPLE = AXC_SPARSE_GAIN_SAMPLE;
 constexpr u32 GS_C = AXC_SPARSE_GAIN_CANDIDATES;
 constexpr u32 GS_TAB = 2 * GS_SAMPLE;                // sample table slots: at most half full
-constexpr u32 GS_BLOCK = 256;
+constexpr u32 GS_BLOCK = 512;
 constexpr size_t GS_SMEM = (size_t)GS_TAB * 16 + (size_t)GS_SAMPLE * 4;  // conn u64, keys u32,
                                                      // inbound u32 per slot; the used-slot list
 // Nodes outside the sampled kernels (gain tiers 0 and 1) have at most GN_BLOCK_W census entries,
@@ -1104,10 +1121,24 @@ __global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const 
             SKey top[GS_C];
 #pragma unroll
             for (u32 r = 0; r < GS_C; ++r) top[r] = SKey{0, 0};
-            for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {
-                const u32 i = used[t], q = keys[i];
-                if (A.psize[q] + s - s / A.discount > A.omega || A.pinb[q] + in_sample - sdc[i] > A.delta) continue;
-                skey_insert(top, SKey{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
+            constexpr u32 U = 4;  // keys per thread whose partition loads are in flight together
+            for (u32 t0 = threadIdx.x; t0 < nd; t0 += U * GS_BLOCK) {
+                u32 qs[U], is[U];
+                u64 ps[U], pb[U];
+#pragma unroll
+                for (u32 r = 0; r < U; ++r) {
+                    const u32 t = t0 + r * GS_BLOCK;
+                    is[r] = t < nd ? used[t] : 0;
+                    qs[r] = t < nd ? keys[is[r]] : NONE;
+                    ps[r] = qs[r] != NONE ? A.psize[qs[r]] : 0;
+                    pb[r] = qs[r] != NONE ? A.pinb[qs[r]] : 0;
+                }
+#pragma unroll
+                for (u32 r = 0; r < U; ++r) {
+                    const u32 q = qs[r], i = is[r];
+                    if (q == NONE || ps[r] + s - s / A.discount > A.omega || pb[r] + in_sample - sdc[i] > A.delta) continue;
+                    skey_insert(top, SKey{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
+                }
             }
             skey_warp_top(top, kred + warp * GS_C);
             __syncthreads();
@@ -1157,7 +1188,7 @@ constexpr u32 CV_WARPS = 4;
 constexpr u32 CV_WARP_LEN = 256;      // longer hyperedges take a block (CS_WARP_CAP)
 constexpr u32 CV_BLOCK_LEN = 4096;    // longer still: a table in device memory (CS_BLOCK_CAP)
 constexpr u32 CV_BLOCK = 256;
-constexpr size_t CV_BLOCK_SMEM = (size_t)2 * CV_BLOCK_LEN * 8;  // keys and values, 2 slots per pin
+constexpr size_t CV_BLOCK_SMEM = (size_t)8 * 8192;  // keys and values of cs_cap(CV_BLOCK_LEN) slots
 
 // Census entries [a, a + lm) of one hyperedge into keys/vals (mask + 1 cleared slots), threads
 // t, t + nt, ...: each partition appears once in a census, so each slot is written once.
@@ -1211,8 +1242,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32) k_cands_warp(GainArgs A, CandAc
     }
     if (!__any_sync(0xFFFFFFFFu, any)) return;
     const u32 lm = A.lam[h];
-    u32 cap = 32;
-    while (cap < 2 * lm) cap <<= 1;
+    const u32 cap = cs_cap(lm);
     u32 *keys = tk[wp], *vals = tv[wp];
     for (u32 i = lane; i < cap; i += 32) keys[i] = NONE;
     __syncwarp();
@@ -1238,8 +1268,11 @@ __global__ void __launch_bounds__(CV_BLOCK) k_cands_block(GainArgs A, CandAcc C,
     for (u64 k = a + threadIdx.x; k < b && !any; k += CV_BLOCK) any = C.spos[A.pins[k]] != NONE;
     if (!__syncthreads_or(any)) return;
     const u32 lm = A.lam[h];
-    u32 cap = 32;
-    while (cap < 2 * lm) cap <<= 1;
+    const u32 cap = cs_cap(lm);
+    if (!gtab && 8ull * cap > dyn_smem_bytes()) {  // launched with too small a table: refuse
+        if (threadIdx.x == 0) atomicExch(A.status, DEV_HASH_FULL);
+        return;
+    }
     u32 *keys = gtab ? gtab + 2 * gtab_off[blockIdx.x] : cv_dyn;
     u32 *vals = keys + cap;
     for (u32 i = threadIdx.x; i < cap; i += CV_BLOCK) keys[i] = NONE;
@@ -2417,6 +2450,10 @@ static LevelPrep prepare_level(Ctx &c, const DLevel &L, const u32 *wfx, u32 K) {
     return lp;
 }
 
+// Longest hyperedge a block-tier table must hold: the level's longest, capped by the tier's bound
+// (the bound itself when the level's is not known).
+static u64 block_tier_len(const LevelPrep &lp, u64 bound) { return lp.max_len && lp.max_len < bound ? lp.max_len : bound; }
+
 static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *part, Census &cs) {
     cs.beg = L.off;
     if (L.e == 0) return;
@@ -2433,7 +2470,8 @@ static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     }
     LAUNCH(c, k_census_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A);
     if (lp.n_hblock)
-        LAUNCH(c, k_census_block, lp.n_hblock, 256, 4 * 2 * CS_BLOCK_CAP * 4, lp.hblock, lp.n_hblock, A,
+        LAUNCH(c, k_census_block, lp.n_hblock, 256, 16 * (size_t)cs_cap(block_tier_len(lp, CS_BLOCK_CAP)),
+               lp.hblock, lp.n_hblock, A,
                (u32 *)nullptr, (const u64 *)nullptr);
     if (lp.n_hhuge) {
         size_t m = c.arena.mark();
@@ -2516,7 +2554,8 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
         LAUNCH(c, k_gain_sample, std::min<u32>(rows, (u32)c.sms), GS_BLOCK, GS_SMEM, A, lp.ntier[2], rows, C);
         LAUNCH(c, k_cands_warp, cdiv(L.e, CV_WARPS), CV_WARPS * 32, 0, A, C, L.e);
         if (lp.n_hblock)
-            LAUNCH(c, k_cands_block, lp.n_hblock, CV_BLOCK, CV_BLOCK_SMEM, A, C, lp.hblock, lp.n_hblock, (u32 *)nullptr,
+            LAUNCH(c, k_cands_block, lp.n_hblock, CV_BLOCK, 8 * (size_t)cs_cap(block_tier_len(lp, CV_BLOCK_LEN)), A,
+                   C, lp.hblock, lp.n_hblock, (u32 *)nullptr,
                    (const u64 *)nullptr);
         if (lp.n_hhuge) {
             u32 *gtab = c.arena.alloc<u32>(2 * lp.huge_tot);
