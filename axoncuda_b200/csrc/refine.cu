@@ -874,9 +874,15 @@ constexpr u32 GS_K = AXC_SPARSE_GAIN_K;
 constexpr u32 GS_SAMPLE = AXC_SPARSE_GAIN_SAMPLE;
 constexpr u32 GS_C = AXC_SPARSE_GAIN_CANDIDATES;
 constexpr u32 GS_TAB = 2 * GS_SAMPLE;                // sample table slots: at most half full
-constexpr u32 GS_BLOCK = 512;
-constexpr size_t GS_SMEM = (size_t)GS_TAB * 16 + (size_t)GS_SAMPLE * 4;  // conn u64, keys u32,
-                                                     // inbound u32 per slot; the used-slot list
+constexpr u32 GS_BLOCK = 256;
+constexpr u32 GS_PER_SM = 2;                         // resident sample blocks per SM
+constexpr u32 GS_DC_BITS = 13;                       // a slot's inbound count (<= GS_SAMPLE) in its low bits
+constexpr u64 GS_DC_MASK = (1ull << GS_DC_BITS) - 1;
+static_assert(GS_SAMPLE <= GS_DC_MASK && GS_DC_BITS + 32 + 13 <= 64 && GS_SAMPLE <= 8192,
+              "packed slot: inbound count below the connectivity (<= GS_SAMPLE u32 weights)");
+static_assert(GS_TAB <= 65536, "used-slot list holds 16-bit slots");
+constexpr size_t GS_SMEM = (size_t)GS_TAB * 12 + (size_t)GS_SAMPLE * 2;  // packed u64 and key u32 per
+                                                     // slot; the used-slot list (u16)
 // Nodes outside the sampled kernels (gain tiers 0 and 1) have at most GN_BLOCK_W census entries,
 // so their sample would be the whole node and the exact kernels give the rule's result.
 static_assert(GN_BLOCK_W <= GS_SAMPLE, "tier-1 nodes must fit the sample");
@@ -1035,21 +1041,20 @@ __device__ __forceinline__ void skey_warp_top(SKey (&top)[GS_C], SKey *out) {
     }
 }
 
-__global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const u32 *__restrict__ list, u32 nl,
+__global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0, const u32 *__restrict__ list, u32 nl,
                                                              CandAcc C) {
     const GainArgs A = gain_args_now(A0);
     extern __shared__ unsigned long long gs_dyn[];
-    unsigned long long *sconn = gs_dyn;      // [GS_TAB]
+    unsigned long long *sacc = gs_dyn;       // [GS_TAB]: sampled connectivity << GS_DC_BITS | inbound count
     u32 *keys = (u32 *)(gs_dyn + GS_TAB);    // [GS_TAB]
-    u32 *sdc = keys + GS_TAB;                // [GS_TAB]
-    u32 *used = sdc + GS_TAB;                // [GS_SAMPLE]: the slots the node filled
+    unsigned short *used = (unsigned short *)(keys + GS_TAB);  // [GS_SAMPLE]: the slots the node filled
     __shared__ unsigned long long wsh[GS_BLOCK / 32];
     __shared__ unsigned long long s_acc;
     __shared__ Cand cred[GS_BLOCK / 32];
     __shared__ SKey kred[(GS_BLOCK / 32) * GS_C];
     __shared__ u32 ndist;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sconn[i] = 0; sdc[i] = 0; }
+    for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sacc[i] = 0; }
     for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
         const u32 u = list[idx], p = A.part[u];
         const u64 t0 = A.toff[u];
@@ -1084,9 +1089,8 @@ __global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const 
             bool fresh = false;
             const u32 slot = hash_insert_fresh(keys, GS_TAB - 1, q, fresh);
             if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
-            if (fresh) used[atomicAdd(&ndist, 1u)] = slot;  // at most GS_SAMPLE distinct keys
-            atomicAdd(&sconn[slot], (unsigned long long)w);
-            if (io && A.cdcnt[k] > 0) atomicAdd(&sdc[slot], 1u);
+            if (fresh) used[atomicAdd(&ndist, 1u)] = (unsigned short)slot;  // at most GS_SAMPLE distinct keys
+            atomicAdd(&sacc[slot], ((unsigned long long)w << GS_DC_BITS) | (io && A.cdcnt[k] > 0 ? 1ull : 0ull));
         };
         if (acc >= (u64)CF_LONG * m)  // few long incidences: one per warp, not 32 per warp
             census_edges(A, u, warp, GS_BLOCK / 32, m, wtot, entry);
@@ -1101,7 +1105,8 @@ __global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const 
             Cand best{INT64_MIN, 0};
             for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {
                 const u32 i = used[t];
-                const Cand c = gain_candidate(A, u, keys[i], sconn[i], sdc[i], saving, wtot);
+                const Cand c = gain_candidate(A, u, keys[i], sacc[i] >> GS_DC_BITS, (u32)(sacc[i] & GS_DC_MASK), saving,
+                                              wtot);
                 if (cand_better(c, best)) best = c;
             }
             best = warp_best(best);
@@ -1136,8 +1141,11 @@ __global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const 
 #pragma unroll
                 for (u32 r = 0; r < U; ++r) {
                     const u32 q = qs[r], i = is[r];
-                    if (q == NONE || ps[r] + s - s / A.discount > A.omega || pb[r] + in_sample - sdc[i] > A.delta) continue;
-                    skey_insert(top, SKey{sconn[i], ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
+                    const u64 v = q == NONE ? 0 : sacc[i];
+                    if (q == NONE || ps[r] + s - s / A.discount > A.omega ||
+                        pb[r] + in_sample - (v & GS_DC_MASK) > A.delta)
+                        continue;
+                    skey_insert(top, SKey{v >> GS_DC_BITS, ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
                 }
             }
             skey_warp_top(top, kred + warp * GS_C);
@@ -1166,8 +1174,7 @@ __global__ void __launch_bounds__(GS_BLOCK, 1) k_gain_sample(GainArgs A0, const 
         for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {  // empty the node's slots for the next one
             const u32 i = used[t];
             keys[i] = NONE;
-            sconn[i] = 0;
-            sdc[i] = 0;
+            sacc[i] = 0;
         }
         __syncthreads();
     }
@@ -2359,6 +2366,8 @@ void setup_refine_kernels(Ctx &c) {
     AXC_CUDA(cudaFuncSetAttribute(k_gain_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * GN_BLOCK_W * 16));
     AXC_CUDA(cudaFuncSetAttribute(k_cascade_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB_DYN_MAX));
     AXC_CUDA(cudaFuncSetAttribute(k_gain_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GS_SMEM));
+    AXC_CUDA(cudaFuncSetAttribute(k_gain_sample, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
     AXC_CUDA(cudaFuncSetAttribute(k_cands_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CV_BLOCK_SMEM));
     AXC_CUDA(cudaFuncSetAttribute(k_rank_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RSS_SMEM));
 }
@@ -2551,7 +2560,7 @@ static void run_gains(Ctx &c, const DLevel &L, const LevelPrep &lp, const GainAr
         C.sacc = c.arena.alloc<unsigned long long>(rows);
         C.wacc = c.arena.alloc<unsigned long long>(rows);
         fill_u32(c, C.spos, NONE, L.n);
-        LAUNCH(c, k_gain_sample, std::min<u32>(rows, (u32)c.sms), GS_BLOCK, GS_SMEM, A, lp.ntier[2], rows, C);
+        LAUNCH(c, k_gain_sample, std::min<u32>(rows, (u32)c.sms * GS_PER_SM), GS_BLOCK, GS_SMEM, A, lp.ntier[2], rows, C);
         LAUNCH(c, k_cands_warp, cdiv(L.e, CV_WARPS), CV_WARPS * 32, 0, A, C, L.e);
         if (lp.n_hblock)
             LAUNCH(c, k_cands_block, lp.n_hblock, CV_BLOCK, 8 * (size_t)cs_cap(block_tier_len(lp, CV_BLOCK_LEN)), A,
