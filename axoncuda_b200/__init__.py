@@ -80,7 +80,7 @@ EXPORTS = [
     "axc_quotient_hgraph_device",
     "axc_gen_snn", "axc_gen_circuit", "axc_submit", "axc_poll", "axc_partition_batch",
     "axc_stage_construct", "axc_stage_rating", "axc_stage_matching", "axc_stage_contract",
-    "axc_stage_gains", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
+    "axc_stage_gains", "axc_stage_refine", "axc_profile_kernel", "axc_profile_read", "axc_connectivity_noalloc",
     "axc_serve_configure", "axc_selftest_bounded_wait", "axc_tune_set",
 ]
 
@@ -131,6 +131,8 @@ def lib() -> C.CDLL:
             "axc_stage_contract": (C.c_int, [C.c_void_p, H, u32p, C.c_uint32, u64p, u32p, u32p, u64p]),
             "axc_stage_gains": (C.c_int, [C.c_void_p, H, u32p, C.c_uint32, u32p, C.c_uint32, C.c_uint32,
                                           C.c_int, C.c_uint32, u32p, i64p]),
+            "axc_stage_refine": (C.c_int, [C.c_void_p, H, u32p, C.c_uint32, u32p, C.c_uint32, C.c_uint32,
+                                           C.c_int, C.c_uint32, C.c_uint64, u32p, u32p]),
         }
         sig["axc_profile_kernel"] = (C.c_int, [C.c_void_p, C.c_char_p])
         sig["axc_profile_read"] = (C.c_int, [C.c_void_p, C.POINTER(KernelTiming)])
@@ -236,13 +238,16 @@ def gen_circuit(n, e, smin=2, smax=64, alpha=2.5, p_local=0.9, local_frac=0.02, 
 
 
 # The workloads: layered SNN (8 x 512, fan-out 64), circuit netlist (200k nodes, 220k nets),
-# large SNN (20 x 50k, lognormal fan-out), each with its run parameters.
+# large SNN (20 x 50k, lognormal fan-out) and its 20 x 5k version, each with its run parameters.
 def workload(name: str) -> tuple[Hypergraph, "Params"]:
     if name == "snn-8x512":
         return gen_snn(8, 512, 64, 0.0, 0, 1.0, 0), params_incc(128, 1024, 1048576, cnc=4, rfr=16, ipm=1)
     if name in ("circuit-200k-k2", "circuit-200k-k64"):
         k = 2 if name.endswith("k2") else 64
         return gen_circuit(200000, 220000, 2, 64, 2.5, 0.9, 0.02, 1), params_kway(k, 0.03, cnc=4, rfr=16)
+    if name == "snn-100k-incc":  # the large SNN's generator at 20 x 5k: a profiling-size INCC case
+        g = gen_snn(20, 5000, 256, 0.8, 2048, 0.7, 2)
+        return g, params_incc(1024, 4096, 1048576, cnc=4, rfr=16, ipm=1)
     if name in ("snn-1m-incc", "snn-1m-k128"):
         g = gen_snn(20, 50000, 256, 0.8, 2048, 0.7, 2)
         if name.endswith("incc"):
@@ -410,3 +415,12 @@ class Context:
                                           _ptr(ns, C.c_uint32), omega, delta, int(encourage), discount,
                                           _ptr(tgt, C.c_uint32), _ptr(gain, C.c_int64)), "axc_stage_gains")
         return tgt[: g.n], gain[: g.n]
+
+    def stage_refine(self, g: Hypergraph, part, num_parts, node_size, omega, delta, encourage, rounds, seed=0):
+        part = np.ascontiguousarray(part, dtype=np.uint32)
+        ns = np.ascontiguousarray(node_size, dtype=np.uint32)
+        out = np.zeros(max(g.n, 1), np.uint32); ran = C.c_uint32()
+        self._check(lib().axc_stage_refine(self._h, C.byref(g.c()), _ptr(part, C.c_uint32), num_parts,
+                                           _ptr(ns, C.c_uint32), omega, delta, int(encourage), rounds, seed,
+                                           _ptr(out, C.c_uint32), C.byref(ran)), "axc_stage_refine")
+        return out[: g.n], ran.value

@@ -880,6 +880,34 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
     }
 }
 
+int axc_stage_refine(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uint32_t num_parts,
+                     const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage, uint32_t rounds,
+                     uint64_t seed, uint32_t *out_part, uint32_t *out_rounds) {
+    if (!ctx || check_graph(g) || !part || !out_part || num_parts == 0) return AXC_EINVAL;
+    for (u32 v = 0; v < g->n; ++v)
+        if (part[v] >= num_parts) return AXC_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Ctx &c = ctx->c;
+    try {
+        const size_t m = c.arena.mark();
+        u32 *wfx;
+        DLevel L = upload_level(c, g, node_size, &wfx);
+        u32 *dp = c.arena.alloc<u32>(g->n ? g->n : 1);
+        if (g->n) AXC_CUDA(cudaMemcpyAsync(dp, part, (size_t)g->n * 4, cudaMemcpyHostToDevice, c.stream));
+        RefineParams rp{num_parts, omega, delta, encourage != 0, rounds, seed};
+        const u32 ran = refine_level(c, L, wfx, rp, dp);
+        if (g->n) AXC_CUDA(cudaMemcpyAsync(out_part, dp, (size_t)g->n * 4, cudaMemcpyDeviceToHost, c.stream));
+        AXC_CUDA(cudaStreamSynchronize(c.stream));
+        if (out_rounds) *out_rounds = ran;
+        c.arena.release(m);
+        return AXC_OK;
+    } catch (const std::exception &e) {
+        cudaStreamSynchronize(c.stream);
+        c.arena.release(0);
+        return guard(ctx, e);
+    }
+}
+
 int axc_selftest_bounded_wait(axc_ctx *ctx, uint32_t spin_limit) {
     if (!ctx || spin_limit == 0) return AXC_EINVAL;
     std::lock_guard<std::mutex> lk(ctx->mu);

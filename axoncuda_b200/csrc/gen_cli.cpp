@@ -2,6 +2,7 @@
 //   axc_gen snn-layered <out> <seed>   8 layers x 512, fan-out 64 from the next layer
 //   axc_gen circuit <out> <seed>       200,000 nodes, 220,000 nets, s^-2.5 on [2,64], 90% within +-2%
 //   axc_gen snn-large <out> <seed>     20 layers x 50,000, fan-out lognormal(256, 0.8) <= 2048, 70% next layer
+//   axc_gen snn-mid <out> <seed>       the same at 20 layers x 5,000
 //   axc_gen snn <out> <layers> <width> <fanout> <sigma> <cap> <p_next> <seed>
 //   axc_gen circ <out> <n> <e> <smin> <smax> <alpha> <p_local> <local_frac> <seed>
 // Built from the generator and writer sources alone (no libaxc.so, no CUDA), so a process that
@@ -15,7 +16,7 @@
 
 int main(int argc, char **argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: axc_gen <snn-layered|circuit|snn-large|snn|circ> <out> ...\n");
+        std::fprintf(stderr, "usage: axc_gen <snn-layered|circuit|snn-large|snn-mid|snn|circ> <out> ...\n");
         return 2;
     }
     std::string kind = argv[1];
@@ -27,6 +28,7 @@ int main(int argc, char **argv) {
     if (kind == "snn-layered") rc = axc_gen_snn(8, 512, 64, 0.0, 0, 1.0, std::strtoull(A(3), 0, 10), &g);
     else if (kind == "circuit") rc = axc_gen_circuit(200000, 220000, 2, 64, 2.5, 0.9, 0.02, std::strtoull(A(3), 0, 10), &g);
     else if (kind == "snn-large") rc = axc_gen_snn(20, 50000, 256, 0.8, 2048, 0.7, std::strtoull(A(3), 0, 10), &g);
+    else if (kind == "snn-mid") rc = axc_gen_snn(20, 5000, 256, 0.8, 2048, 0.7, std::strtoull(A(3), 0, 10), &g);
     else if (kind == "snn")
         rc = axc_gen_snn(std::atoi(A(3)), std::atoi(A(4)), std::atof(A(5)), std::atof(A(6)), std::atoi(A(7)),
                          std::atof(A(8)), std::strtoull(A(9), 0, 10), &g);

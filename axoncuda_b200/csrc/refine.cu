@@ -878,6 +878,7 @@ constexpr u32 GS_BLOCK = 256;
 constexpr u32 GS_PER_SM = 2;                         // resident sample blocks per SM
 constexpr u32 GS_DC_BITS = 13;                       // a slot's inbound count (<= GS_SAMPLE) in its low bits
 constexpr u64 GS_DC_MASK = (1ull << GS_DC_BITS) - 1;
+constexpr u64 GS_RULED_OUT = 1ull << 63;             // slot mark: the size or inbound bound rules it out
 static_assert(GS_SAMPLE <= GS_DC_MASK && GS_DC_BITS + 32 + 13 <= 64 && GS_SAMPLE <= 8192,
               "packed slot: inbound count below the connectivity (<= GS_SAMPLE u32 weights)");
 static_assert(GS_TAB <= 65536, "used-slot list holds 16-bit slots");
@@ -963,23 +964,6 @@ __device__ __forceinline__ void census_flat(const GainArgs &A, u32 u, u32 first,
     }
 }
 
-// Census entries of u's incidences j = first, first + stride, ... below jend, one incidence per
-// warp at a time (the calling warp's `first` and `stride` are multiples of one incidence): for
-// nodes whose few incidences have long entry lists. Same calls as census_flat; lane 0 adds each
-// incidence's weight to wtot.
-template <class F>
-__device__ __forceinline__ void census_edges(const GainArgs &A, u32 u, u32 first, u32 stride, u32 jend, i64 &wtot,
-                                             F &&f) {
-    const u64 t0 = A.toff[u];
-    const u32 nin_u = A.nin[u];
-    for (u32 j = first; j < jend; j += stride) {
-        const u32 h = A.touch[t0 + j];
-        const u32 w = A.wfx[h];
-        if ((threadIdx.x & 31u) == 0) wtot += w;
-        census_edge_warp(A, A.off[h], A.lam[h], w, j < nin_u ? 1u : 0u, f);
-    }
-}
-
 // Block-wide sum of a u64 over GS_BLOCK threads (every thread gets it). `sh` holds one word per warp.
 __device__ __forceinline__ u64 block_sum_u64(u64 v, unsigned long long *sh) {
     v = warp_sum(v);
@@ -1053,6 +1037,10 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
     __shared__ Cand cred[GS_BLOCK / 32];
     __shared__ SKey kred[(GS_BLOCK / 32) * GS_C];
     __shared__ u32 ndist;
+    // the first GS_BLOCK incidences: exclusive census prefix (entry GS_BLOCK or m = the sample's
+    // total), census offset and weight
+    __shared__ u32 s_ex[GS_BLOCK + 1], s_w[GS_BLOCK];
+    __shared__ u64 s_off[GS_BLOCK];
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (u32 i = threadIdx.x; i < GS_TAB; i += GS_BLOCK) { keys[i] = NONE; sacc[i] = 0; }
     for (u32 idx = blockIdx.x; idx < nl; idx += gridDim.x) {
@@ -1065,7 +1053,13 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
         u64 acc = 0;
         for (u32 base = 0; base < deg; base += GS_BLOCK) {
             const u32 j = base + threadIdx.x;
-            u64 x = j < deg ? (u64)A.lam[A.touch[t0 + j]] : 0;
+            const u32 h = j < deg ? A.touch[t0 + j] : 0;
+            const u32 lm = j < deg ? A.lam[h] : 0;
+            if (base == 0 && j < deg) {
+                s_off[j] = A.off[h];
+                s_w[j] = A.wfx[h];
+            }
+            u64 x = lm;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const u64 y = __shfl_up_sync(0xFFFFFFFFu, x, o);
@@ -1074,6 +1068,7 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
             if (lane == 31) wsh[warp] = x;
             __syncthreads();
             for (u32 i = 0; i < warp; ++i) x += wsh[i];
+            if (base == 0) s_ex[threadIdx.x] = (u32)(x - lm < GS_SAMPLE ? x - lm : GS_SAMPLE);  // exact for j < m
             const bool take = j < deg && acc + x <= GS_SAMPLE;
             const u32 cnt = (u32)__syncthreads_count(take);
             if (cnt > 0 && threadIdx.x == cnt - 1) s_acc = acc + x;
@@ -1082,20 +1077,47 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
             if (cnt > 0) acc = s_acc;
             if (cnt < GS_BLOCK) break;
         }
+        if (threadIdx.x == 0 && m <= GS_BLOCK) s_ex[m] = (u32)acc;
+        __syncthreads();
         // 2. sampled connectivity; saving and wtot are exact when the sample is the whole node
         i64 saving = 0, wtot = 0;
-        const auto entry = [&](u64 k, u32 q, u32 w, u32 io) {
+        const auto put = [&](u64 k, u32 q, u32 w, bool dst) {
             if (q == p) { saving += leave_gain(A.encourage, w, A.ccnt[k]); return; }
             bool fresh = false;
             const u32 slot = hash_insert_fresh(keys, GS_TAB - 1, q, fresh);
             if (slot == NONE) { atomicExch(A.status, DEV_HASH_FULL); return; }
             if (fresh) used[atomicAdd(&ndist, 1u)] = (unsigned short)slot;  // at most GS_SAMPLE distinct keys
-            atomicAdd(&sacc[slot], ((unsigned long long)w << GS_DC_BITS) | (io && A.cdcnt[k] > 0 ? 1ull : 0ull));
+            atomicAdd(&sacc[slot], ((unsigned long long)w << GS_DC_BITS) | (dst ? 1ull : 0ull));
         };
-        if (acc >= (u64)CF_LONG * m)  // few long incidences: one per warp, not 32 per warp
-            census_edges(A, u, warp, GS_BLOCK / 32, m, wtot, entry);
-        else
-            census_flat(A, u, 32 * warp, GS_BLOCK, m, wtot, entry);
+        if (m <= GS_BLOCK) {
+            // the sample's acc entries split evenly over the block: thread t takes entries t,
+            // t + GS_BLOCK, ..., finding each one's incidence with a cursor over s_ex
+            constexpr u32 U = 4;
+            u32 j = 0;
+            for (u32 f0 = threadIdx.x; f0 < acc; f0 += U * GS_BLOCK) {
+                u64 kk[U];
+                u32 xx[U], jj[U], dd[U];
+#pragma unroll
+                for (u32 r = 0; r < U; ++r) {
+                    const u32 f = f0 + r * GS_BLOCK;
+                    jj[r] = NONE;
+                    if (f < acc) {
+                        while (s_ex[j + 1] <= f) ++j;  // s_ex[m] = acc > f ends it below m
+                        jj[r] = j;
+                        kk[r] = s_off[j] + (f - s_ex[j]);
+                        xx[r] = A.cpart[kk[r]];
+                        dd[r] = j < nin_u ? A.cdcnt[kk[r]] : 0;
+                    }
+                }
+#pragma unroll
+                for (u32 r = 0; r < U; ++r)
+                    if (jj[r] != NONE) put(kk[r], xx[r], s_w[jj[r]], dd[r] > 0);
+            }
+            if (threadIdx.x < m) wtot = s_w[threadIdx.x];
+        } else {
+            census_flat(A, u, 32 * warp, GS_BLOCK, m, wtot,
+                        [&](u64 k, u32 q, u32 w, u32 io) { put(k, q, w, io && q != p && A.cdcnt[k] > 0); });
+        }
         __syncthreads();
         const u32 nd = ndist;
         const u64 s = A.nsize[u];
@@ -1120,12 +1142,12 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
             }
         } else {
             // 3b. the GS_C best by (sampled connectivity, tie hash, -id) among the keys the size
-            // limit and the inbound bound do not rule out: per-thread lists, then per warp, then
-            // warp 0 over the warps' lists
+            // limit and the inbound bound do not rule out. Pass 1 marks the ruled-out slots and
+            // takes each warp's best key; the least of those GS_BLOCK / 32 >= GS_C keys is no
+            // better than the GS_C-th best, so pass 2 lists only the keys at or above it
+            // (per-thread lists, then per warp, then warp 0 over the warps' lists).
             const u64 in_sample = m < nin_u ? m : nin_u;
-            SKey top[GS_C];
-#pragma unroll
-            for (u32 r = 0; r < GS_C; ++r) top[r] = SKey{0, 0};
+            SKey best1{0, 0};
             constexpr u32 U = 4;  // keys per thread whose partition loads are in flight together
             for (u32 t0 = threadIdx.x; t0 < nd; t0 += U * GS_BLOCK) {
                 u32 qs[U], is[U];
@@ -1141,12 +1163,37 @@ __global__ void __launch_bounds__(GS_BLOCK, GS_PER_SM) k_gain_sample(GainArgs A0
 #pragma unroll
                 for (u32 r = 0; r < U; ++r) {
                     const u32 q = qs[r], i = is[r];
-                    const u64 v = q == NONE ? 0 : sacc[i];
-                    if (q == NONE || ps[r] + s - s / A.discount > A.omega ||
-                        pb[r] + in_sample - (v & GS_DC_MASK) > A.delta)
+                    if (q == NONE) continue;
+                    const u64 v = sacc[i];
+                    if (ps[r] + s - s / A.discount > A.omega || pb[r] + in_sample - (v & GS_DC_MASK) > A.delta) {
+                        sacc[i] = v | GS_RULED_OUT;
                         continue;
-                    skey_insert(top, SKey{v >> GS_DC_BITS, ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)});
+                    }
+                    const SKey k{v >> GS_DC_BITS, ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)};
+                    if (skey_better(k, best1)) best1 = k;
                 }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const SKey c{__shfl_xor_sync(0xFFFFFFFFu, best1.hi, o), __shfl_xor_sync(0xFFFFFFFFu, best1.lo, o)};
+                if (skey_better(c, best1)) best1 = c;
+            }
+            if (lane == 0) kred[warp] = best1;
+            __syncthreads();
+            SKey thr = kred[0];
+            for (u32 w2 = 1; w2 < GS_BLOCK / 32; ++w2)
+                if (skey_better(thr, kred[w2])) thr = kred[w2];
+            __syncthreads();  // kred is reused below
+            SKey top[GS_C];
+#pragma unroll
+            for (u32 r = 0; r < GS_C; ++r) top[r] = SKey{0, 0};
+            for (u32 t = threadIdx.x; t < nd; t += GS_BLOCK) {
+                const u32 i = used[t];
+                const u64 v = sacc[i];
+                if (v & GS_RULED_OUT) continue;
+                const u32 q = keys[i];
+                const SKey k{v >> GS_DC_BITS, ((u64)mix32(q + A.round + A.seed) << 32) | (u64)(~q)};
+                if (!skey_better(thr, k)) skey_insert(top, k);
             }
             skey_warp_top(top, kred + warp * GS_C);
             __syncthreads();
@@ -1714,6 +1761,11 @@ constexpr u32 CB_THREADS = 128;
 constexpr u32 CB_MOV_MAX = 2048;  // movers of the block kernel, in shared memory
 constexpr u32 CB_TAB_HASH = 8192; // hashed table slots of the block kernel, at most
 constexpr size_t CB_DYN_MAX = (size_t)CB_MOV_MAX * 12 + (size_t)CB_TAB_HASH * 12;
+// The block kernel's middle tier (hashed tables): hyperedges with at most CB_MID_MOV movers and
+// CB_MID_TAB table slots take blocks small enough for several per SM; the rest go on to the
+// launch sized by the level's largest hyperedge.
+constexpr u32 CB_MID_MOV = 512;
+constexpr u32 CB_MID_TAB = 2048;
 
 // Gather the movers of hyperedge h (rank << 32 | dst flag | node) into mvs[0, min(m, lim)) with
 // the whole block; returns m (all of them, counted past lim) and their largest rank in *rmax.
@@ -2712,10 +2764,11 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     A.dyn = dyn;
     run_gains(c, L, lp, A, cs);
     // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
-    // [3] cascade hyperedges for the block kernel, [4] for the scratch kernel
+    // [3] cascade hyperedges for the block kernel, [4] for the scratch kernel, [5] for the block
+    // kernel's full-size launch after its middle tier
     u32 *cnt = c.arena.alloc<u32>(8);
     AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
-    u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4;
+    u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4, *dBig2 = cnt + 5;
     // small levels: ranking, validity and the best prefix in one block each (SMALL_*)
     const bool small = rp.K <= VS_MAX_K && n <= (u32)RSS_CAP && rp.copies == 1;
     // movers in id order, then ranked by (gain desc, id asc)
@@ -2796,6 +2849,7 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         const bool direct = rp.K <= CC_DIRECT_K;
         size_t m1 = c.arena.mark();
         u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1), *huge = c.arena.alloc<u32>(L.e ? L.e : 1);
+        u32 *big2 = c.arena.alloc<u32>(L.e ? L.e : 1);
         if (L.e) {
             LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
             // block kernel: shared memory sized by the level's largest hyperedge, all resident blocks
@@ -2806,11 +2860,22 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
                                     : (u32)std::min<u64>(cascade_cap(std::min<u64>(lp.max_len, rp.K),
                                                                      std::min<u64>(lp.max_len, smov)),
                                                          CB_TAB_HASH);
+            const u32 *blist = big, *bcount = dBig;
+            if (!direct && (smov > CB_MID_MOV || stab > CB_MID_TAB)) {  // middle tier first
+                const u32 smid = std::min(smov, CB_MID_MOV), tmid = std::min(stab, CB_MID_TAB);
+                const size_t dmid = (size_t)smid * 12 + (size_t)tmid * 12;
+                int per_mid = 1;
+                AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_mid, k_cascade_block, CB_THREADS, dmid));
+                LAUNCH(c, k_cascade_block, (u32)c.sms * (u32)std::max(per_mid, 1), CB_THREADS, dmid, C, big, dBig, smid,
+                       tmid, big2, dBig2);
+                blist = big2;
+                bcount = dBig2;
+            }
             const size_t dyn = (size_t)smov * 12 + (size_t)stab * 12;
             int per_sm = 1;
             AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cascade_block, CB_THREADS, dyn));
             const u32 grid = (u32)c.sms * (u32)std::max(per_sm, 1);
-            LAUNCH(c, k_cascade_block, grid, CB_THREADS, dyn, C, big, dBig, smov, stab, huge, dHuge);
+            LAUNCH(c, k_cascade_block, grid, CB_THREADS, dyn, C, blist, bcount, smov, stab, huge, dHuge);
             // scratch kernel, only when some hyperedge can outgrow the block kernel: one slice of
             // movers, slots and tables per block, at most 1 GiB in all
             u64 mv_cap = 1;
@@ -2999,7 +3064,7 @@ static u32 refine_level_loop(Ctx &c, const DLevel &L, const LevelPrep &lp, const
     u32 *dyn = c.arena.alloc<u32>(2), *rs = c.arena.alloc<u32>(4);
     {
         u32 *hp = (u32 *)((char *)c.h_pinned + 64);
-        hp[0] = 1u;  // discount of round 0 (R >= 2, so round 0 is in the first third)
+        hp[0] = 0 < R / 3 ? 1u : (0 < 2 * R / 3 ? 2u : 0xFFFFFFFFu);  // discount of round 0 (2 when R = 2)
         hp[1] = 0u;
         hp[2] = 0u;  // rs: r, R, rounds done
         hp[3] = R;

@@ -60,6 +60,12 @@ WORKLOADS = {
         gen=("snn-large", "2", ".snn"), kway=False,
         ref=["-m", "1024", "4096", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"],
         grade=["-m-prt", "1024", "4096", "1048576"]),
+    "snn-100k-incc": dict(
+        desc="SNN 20x5k lognormal fan-out seed 2 (the large SNN's generator at a tenth of the width), INCC "
+             "omega=1024 delta=4096 Kmax=1048576: a profiling-size case",
+        gen=("snn-mid", "2", ".snn"), kway=False,
+        ref=["-m", "1024", "4096", "1048576", "-rfr", "16", "-cnc", "4", "-dtc", "-ipm", "-v", "0"],
+        grade=["-m-prt", "1024", "4096", "1048576"]),
     "snn-1m-k128": dict(
         desc="large SNN 20x50k lognormal fan-out seed 2, k-way k=128 eps=0.03",
         gen=("snn-large", "2", ".snn"), kway=True,

@@ -312,6 +312,16 @@ int axc_stage_gains(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uin
                     const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage,
                     uint32_t discount, uint32_t *out_target, int64_t *out_gain);
 
+/* All refinement rounds of one level for a given partition: the rounds of refinementRepeats
+ * (sources/refinement.cu:82-545): gains, cascade, size and inbound validity, best prefix and apply,
+ * `rounds` rounds under the skip schedule (discount 1, 2, none by thirds; a round without moves
+ * skips ahead, sources/refinement.cu:536-543). Arguments as axc_stage_gains, plus the round count
+ * and the seed of the tie hash; out_part[n] receives the refined partition (ids below num_parts)
+ * and *out_rounds the rounds that ran. */
+int axc_stage_refine(axc_ctx *ctx, const axc_hgraph *g, const uint32_t *part, uint32_t num_parts,
+                     const uint32_t *node_size, uint32_t omega, uint32_t delta, int encourage,
+                     uint32_t rounds, uint64_t seed, uint32_t *out_part, uint32_t *out_rounds);
+
 /* ---- failure path of the bounded device waits (no reference counterpart: the reference's waits
  * are grid syncs and host synchronizations, which never time out) ------------------------------------
  * Runs one look-back wait of the single-pass scans (the only waits on other blocks' flags in this

@@ -999,6 +999,21 @@ void or_gains(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
     gains(rc, pv, cs, ps, pi, discount, round, target, gain);
 }
 
+void or_refine(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins, const uint32_t *nsrc,
+               const uint32_t *wfx, const uint64_t *toff, const uint32_t *touch, const uint32_t *inbound,
+               const uint32_t *node_size, uint32_t *part, uint32_t num_parts, uint32_t omega, uint32_t delta,
+               int encourage, uint32_t rounds, uint64_t seed) {
+    G g = mkG(n, e, off, pins, nsrc);
+    T t;
+    t.toff.assign(toff, toff + n + 1);
+    t.touch.assign(touch, touch + toff[n]);
+    t.nin.assign(inbound, inbound + n);
+    std::vector<u32> w(wfx, wfx + e), pv(part, part + n);
+    RefineCtx rc{&g, &t, &w, node_size, num_parts, omega, delta, encourage != 0, seed};
+    refine_level(rc, pv, rounds);
+    std::copy(pv.begin(), pv.end(), part);
+}
+
 void or_evaluate(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
                  const uint32_t *nsrc, const float *w, const uint32_t *part, uint32_t omega,
                  uint32_t delta, uint32_t max_parts, int64_t *out) {

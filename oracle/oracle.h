@@ -71,6 +71,11 @@ void or_gains(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
  * sources/constr.cpp:90-147), all exact in fixed point.
  * out[0]=connectivity_fx out[1]=cutnet_fx out[2]=soed_fx out[3]=num_parts out[4]=max_size
  * out[5]=max_inbound out[6]=valid(0/1) out[7]=ids_dense(0/1). */
+// refine_level (sources/refinement.cu:82-545) on a given partition, updated in place
+void or_refine(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins, const uint32_t *nsrc,
+               const uint32_t *wfx, const uint64_t *toff, const uint32_t *touch, const uint32_t *inbound,
+               const uint32_t *node_size, uint32_t *part, uint32_t num_parts, uint32_t omega, uint32_t delta,
+               int encourage, uint32_t rounds, uint64_t seed);
 void or_evaluate(uint32_t n, uint32_t e, const uint64_t *off, const uint32_t *pins,
                  const uint32_t *nsrc, const float *w, const uint32_t *part, uint32_t omega,
                  uint32_t delta, uint32_t max_parts, int64_t *out);

@@ -140,6 +140,20 @@ def gains(n, off, pins, nsrc, wfx_, node_size, part, num_parts, omega, delta, en
     return tgt[:n], gain[:n]
 
 
+def refine(n, off, pins, nsrc, wfx_, node_size, part, num_parts, omega, delta, encourage, rounds, seed=0):
+    off, pins, nsrc, wfx_, ns = _u64(off), _u32(pins), _u32(nsrc), _u32(wfx_), _u32(node_size)
+    toff, touch, nin = touching(n, off, pins, nsrc)
+    pv = np.array(part, dtype=np.uint32, copy=True)
+    if len(pv) == 0:
+        pv = np.zeros(1, np.uint32)
+    lib().or_refine(C.c_uint32(n), C.c_uint32(len(nsrc)), _p(off, C.c_uint64), _p(pins, C.c_uint32),
+                    _p(nsrc, C.c_uint32), _p(wfx_, C.c_uint32), _p(toff, C.c_uint64), _p(touch, C.c_uint32),
+                    _p(nin, C.c_uint32), _p(ns, C.c_uint32), _p(pv, C.c_uint32), C.c_uint32(num_parts),
+                    C.c_uint32(omega), C.c_uint32(delta), C.c_int(int(encourage)), C.c_uint32(rounds),
+                    C.c_uint64(seed))
+    return pv[:n]
+
+
 def evaluate(n, off, pins, nsrc, w, part, omega, delta, max_parts):
     off, pins, nsrc, part = _u64(off), _u32(pins), _u32(nsrc), _u32(part)
     w = np.ascontiguousarray(w, dtype=np.float32)

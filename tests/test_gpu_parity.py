@@ -170,6 +170,51 @@ def test_cascade_kernels_match_oracle(ctx, monkeypatch, i, block_movers):
         assert st.num_parts > 256
 
 
+# Whole refinement levels (axc_stage_refine against the oracle's refine_level): every round count
+# from 1 (one eager round) to 6 (rounds replayed on the device), INCC and k-way. R = 2 starts in
+# the schedule's second third (discount 2) and R = 3 in the first.
+REFINE_CASES = [("snn_5x40_ln.snn", True, 24, 12, 60), ("circ_2k.hgr", False, 8, 600, 1 << 20)]
+
+
+@pytest.mark.parametrize("rounds", [1, 2, 3, 6])
+@pytest.mark.parametrize("name,encourage,K,omega,delta", REFINE_CASES)
+def test_refine_rounds_match_oracle(ctx, name, encourage, K, omega, delta, rounds):
+    g = dedup(golden(name))
+    rng = np.random.default_rng(rounds)
+    part = rng.integers(0, K, g.n).astype(np.uint32)
+    ns = rng.integers(1, 3, g.n).astype(np.uint32)
+    out, ran = ctx.stage_refine(g, part, K, ns, omega, delta, encourage, rounds, 3)
+    o = O.refine(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, part, K, omega, delta, encourage, rounds, 3)
+    np.testing.assert_array_equal(out, o)
+    assert 1 <= ran <= rounds and (out != part).any()
+
+
+def test_refine_two_rounds_discount_matches_oracle(ctx):
+    """Two rounds from a refined partition in which every node has a move: round 0 runs at
+    discount 2, and the oracle applies one move in each round."""
+    g0 = ax.gen_snn(3, 900, 650, 0.25, 1100, 1.0, 41)
+    g = dedup(g0)
+    start, K, _, _ = oracle_partition(g0, ax.params_incc(8, 2048, 1048576, cnc=4, rfr=1))
+    ns = np.ones(g.n, np.uint32)
+    out, ran = ctx.stage_refine(g, start, K, ns, 8, 2048, 1, 2)
+    o = O.refine(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, start, K, 8, 2048, 1, 2)
+    np.testing.assert_array_equal(out, o)
+    assert ran == 2 and (o != start).sum() == 2
+
+
+# Hashed cascade tables with hyperedges of up to 1101 pins: the block kernel's middle tier (at most
+# 512 movers and 2048 table slots) takes the mid-size hyperedges and hands the larger ones to the
+# launch sized by the level's longest hyperedge.
+def test_cascade_middle_tier_matches_oracle(ctx):
+    g = ax.gen_snn(3, 900, 650, 0.25, 1100, 1.0, 41)
+    assert np.diff(g.off.astype(np.int64)).max() > 1024
+    p = ax.params_incc(8, 2048, 1048576, cnc=4, rfr=2)
+    part, st = ctx.partition(g, p)
+    o_part, o_K, _, _ = oracle_partition(g, p)
+    np.testing.assert_array_equal(part, o_part)
+    assert st.valid == 1 and st.num_parts > 256
+
+
 # Nodes whose gain-table bound passes 4096 slots (here about 2000 partitions of two neurons and
 # about 80 inbound hyperedges of about 80 pins) first try a shared-memory table and fall back to a
 # global one when they reach too many distinct partitions. With at most 4096 partitions the first
