@@ -108,6 +108,9 @@ struct Ctx {
     u32 prof_launches = 0;
     bool capturing = false;
     bool profiling(const char *name) const { return prof_on && prof_name == name; }
+    // Device-side byte counter of the kernels whose algorithmic bytes depend on device data (they
+    // add them while profiled): a word of the status allocation, read and cleared by profile reads.
+    unsigned long long *d_prof_bytes() const { return (unsigned long long *)((char *)d_status + 64); }
     cudaEvent_t prof_event() {
         if (prof_used == prof_ev.size()) {
             cudaEvent_t e;

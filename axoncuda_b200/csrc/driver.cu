@@ -333,6 +333,7 @@ int axc_profile_kernel(axc_ctx *ctx, const char *kernel) {
     c.prof_bytes = 0;
     c.prof_ms = 0;
     c.prof_launches = 0;
+    if (c.d_status && cudaMemset(c.d_prof_bytes(), 0, 8) != cudaSuccess) return AXC_ECUDA;
     return AXC_OK;
 }
 
@@ -343,9 +344,12 @@ int axc_profile_read(axc_ctx *ctx, axc_kernel_timing *out) {
     try {
         AXC_CUDA(cudaStreamSynchronize(c.stream));
         c.prof_collect(0, c.prof_used);
+        unsigned long long dev_bytes = 0;  // bytes the profiled kernel counted on the device
+        AXC_CUDA(cudaMemcpy(&dev_bytes, c.d_prof_bytes(), 8, cudaMemcpyDeviceToHost));
+        AXC_CUDA(cudaMemset(c.d_prof_bytes(), 0, 8));
         out->launches = c.prof_launches;
         out->ms_total = c.prof_ms;
-        out->bytes = c.prof_bytes;
+        out->bytes = c.prof_bytes + dev_bytes;
         c.prof_used = 0;
         c.prof_bytes = 0;
         c.prof_ms = 0;

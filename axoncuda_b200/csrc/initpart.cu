@@ -24,15 +24,22 @@ __global__ void k_bfs_expand(const u32 *__restrict__ front, u32 nf, u32 level, c
     const u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= nf) return;
     const u32 u = front[i];
-    for (u64 j = toff[u]; j < toff[u + 1]; ++j) {
-        const u32 h = touch[j];
-        u32 claim = 0;
-        if (lane == 0) claim = atomicExch(&hdone[h], 1u);
-        claim = __shfl_sync(0xFFFFFFFFu, claim, 0);
-        if (claim) continue;
-        for (u64 k = off[h] + lane; k < off[h + 1]; k += 32) {
-            const u32 v = pins[k];
-            if (atomicCAS(&dist[v], NONE, level + 1) == NONE) next[atomicAdd(nn, 1u)] = v;
+    const u64 jend = toff[u + 1];
+    // 32 incidences claimed at once (one per lane), then each claimed hyperedge expanded by the
+    // whole warp; the distances do not depend on the order
+    for (u64 jb = toff[u]; jb < jend; jb += 32) {
+        const u64 j = jb + lane;
+        const u32 h = j < jend ? touch[j] : 0;
+        const bool mine = j < jend && atomicExch(&hdone[h], 1u) == 0;
+        u32 bal = __ballot_sync(0xFFFFFFFFu, mine);
+        while (bal) {
+            const u32 t = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const u32 hh = __shfl_sync(0xFFFFFFFFu, h, t);
+            for (u64 k = off[hh] + lane; k < off[hh + 1]; k += 32) {
+                const u32 v = pins[k];
+                if (atomicCAS(&dist[v], NONE, level + 1) == NONE) next[atomicAdd(nn, 1u)] = v;
+            }
         }
     }
 }

@@ -1494,6 +1494,8 @@ struct CascadeArgs {
     u32 dense_stride;
     u32 *status;
     u32 K;  // partitions: with K <= CC_DIRECT_K the per-hyperedge tables are indexed by partition id
+    // when set (kernel timer on k_cascade_warp): each hyperedge's algorithmic bytes are added here
+    unsigned long long *pbytes;
 };
 
 constexpr u32 MV_DST = 0x80000000u;  // mover flag in the node field: the pin is a destination
@@ -1683,59 +1685,85 @@ __device__ void cascade_sweep_warp(const CascadeArgs &A, u32 h, const u64 *mv, c
     }
 }
 
-__global__ void k_cascade_warp(CascadeArgs A, u32 *__restrict__ big, u32 *__restrict__ nbig) {
+// The hyperedges that hold a mover: every incidence of every mover flags its hyperedge (flag[]
+// zeroed before), then the flags are compacted into the cascade's list. One warp per mover.
+__global__ void k_mover_hedges(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u64 *__restrict__ toff,
+                               const u32 *__restrict__ touch, u32 *__restrict__ flag) {
+    const u32 lane = threadIdx.x & 31u, nw = (gridDim.x * blockDim.x) >> 5;
+    const u32 M = *dM;
+    for (u32 r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < M; r += nw) {
+        const u32 u = mv[r];
+        for (u64 j = toff[u] + lane; j < toff[u + 1]; j += 32) flag[touch[j]] = 1u;
+    }
+}
+
+__global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, const u32 *__restrict__ nlist,
+                               u32 *__restrict__ big, u32 *__restrict__ nbig) {
     __shared__ u64 mvs[CC_WARPS][CC_MOV];
     __shared__ u32 sl[CC_WARPS][CC_MOV];
     __shared__ u32 tk[CC_WARPS][CC_TAB], tc[CC_WARPS][CC_TAB], td[CC_WARPS][CC_TAB];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u32 h = blockIdx.x * CC_WARPS + w;
-    if (h >= A.e) return;
-    const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
-    // collect movers (rank << 32 | dst flag | node)
-    u32 m = 0;
-    for (u64 base = a; base < b; base += 32) {
-        u64 k = base + lane;
-        u32 v = k < b ? A.pins[k] : 0, r = k < b ? A.rank[v] : NONE;
-        bool mvr = r != NONE;
-        u32 bal = __ballot_sync(0xFFFFFFFFu, mvr);
-        if (mvr) {
-            u32 pos = m + __popc(bal & ((1u << lane) - 1u));
-            if (pos < CC_MOV) mvs[w][pos] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
+    const u32 nl = *nlist;
+    for (u32 idx = blockIdx.x * CC_WARPS + w; idx < nl; idx += gridDim.x * CC_WARPS) {
+        __syncwarp();  // the previous hyperedge's shared state is no longer read
+        const u32 h = list[idx];
+        const u64 a = A.off[h], b = A.off[h + 1], d0 = a + A.nsrc[h];
+        // collect movers (rank << 32 | dst flag | node)
+        u32 m = 0;
+        for (u64 base = a; base < b; base += 32) {
+            u64 k = base + lane;
+            u32 v = k < b ? A.pins[k] : 0, r = k < b ? A.rank[v] : NONE;
+            bool mvr = r != NONE;
+            u32 bal = __ballot_sync(0xFFFFFFFFu, mvr);
+            if (mvr) {
+                u32 pos = m + __popc(bal & ((1u << lane) - 1u));
+                if (pos < CC_MOV) mvs[w][pos] = ((u64)r << 32) | (k >= d0 ? MV_DST : 0u) | v;
+            }
+            m += __popc(bal);
         }
-        m += __popc(bal);
+        // algorithmic bytes (kernel timer): the list entry, offsets and source count, each pin's id
+        // and rank, the census size, then the hand-off to the block kernel or the census entries,
+        // each mover's partition, target and cascaded gain, and the weight (transitions not counted)
+        const u64 bytes_read = 24 + 8 * (b - a);
+        if (m == 0) {  // (a listed hyperedge always has a mover)
+            if (A.pbytes && lane == 0) atomicAdd(A.pbytes, (unsigned long long)bytes_read);
+            continue;
+        }
+        const u32 lm = A.lam[h];
+        const bool direct = cascade_direct(A);
+        const u32 cap = direct ? A.K : cascade_cap32(lm, m);
+        if (m > CC_MOV || cap > CC_TAB) {
+            if (lane == 0) big[atomicAdd(nbig, 1u)] = h;  // handled by the block kernel
+            if (A.pbytes && lane == 0) atomicAdd(A.pbytes, (unsigned long long)(bytes_read + 8));
+            continue;
+        }
+        if (A.pbytes && lane == 0)
+            atomicAdd(A.pbytes, (unsigned long long)(bytes_read + 8 + 12ull * lm + 16ull * m));
+        __syncwarp();
+        // sort movers by rank: each key's position is the number of smaller keys (keys are unique)
+        u64 mine[CC_MOV / 32];
+        u32 posv[CC_MOV / 32];
+        for (u32 i = 0; i < CC_MOV / 32; ++i) mine[i] = (lane + 32 * i < m) ? mvs[w][lane + 32 * i] : ~0ull;
+        for (u32 i = 0; i < CC_MOV / 32; ++i) {
+            posv[i] = 0;
+            if (lane + 32 * i >= m) continue;
+            for (u32 j = 0; j < m; ++j) posv[i] += mvs[w][j] < mine[i];
+        }
+        __syncwarp();
+        for (u32 i = 0; i < CC_MOV / 32; ++i)
+            if (lane + 32 * i < m) mvs[w][posv[i]] = mine[i];
+        // table of partition counts from the census, then the movers' slots; direct tables leave
+        // tk to the sweep's lane masks (2K <= CC_TAB words, zeroed)
+        for (u32 i = lane; i < cap; i += 32) { tc[w][i] = 0; td[w][i] = 0; }
+        const u32 ntk = direct ? 2 * A.K : cap;
+        for (u32 i = lane; i < ntk; i += 32) tk[w][i] = direct ? 0u : NONE;
+        __syncwarp();
+        cascade_fill(A, a, lm, tk[w], tc[w], td[w], cap, lane, 32);
+        __syncwarp();
+        cascade_slots(A, mvs[w], sl[w], m, tk[w], cap, lane, 32);
+        __syncwarp();
+        cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], direct ? tk[w] : nullptr);
     }
-    if (m == 0) return;
-    const u32 lm = A.lam[h];
-    const bool direct = cascade_direct(A);
-    const u32 cap = direct ? A.K : cascade_cap32(lm, m);
-    if (m > CC_MOV || cap > CC_TAB) {
-        if (lane == 0) big[atomicAdd(nbig, 1u)] = h;  // handled by the block kernel
-        return;
-    }
-    __syncwarp();
-    // sort movers by rank: each key's position is the number of smaller keys (keys are unique)
-    u64 mine[CC_MOV / 32];
-    u32 posv[CC_MOV / 32];
-    for (u32 i = 0; i < CC_MOV / 32; ++i) mine[i] = (lane + 32 * i < m) ? mvs[w][lane + 32 * i] : ~0ull;
-    for (u32 i = 0; i < CC_MOV / 32; ++i) {
-        posv[i] = 0;
-        if (lane + 32 * i >= m) continue;
-        for (u32 j = 0; j < m; ++j) posv[i] += mvs[w][j] < mine[i];
-    }
-    __syncwarp();
-    for (u32 i = 0; i < CC_MOV / 32; ++i)
-        if (lane + 32 * i < m) mvs[w][posv[i]] = mine[i];
-    // table of partition counts from the census, then the movers' slots; direct tables leave tk
-    // to the sweep's lane masks (2K <= CC_TAB words, zeroed)
-    for (u32 i = lane; i < cap; i += 32) { tc[w][i] = 0; td[w][i] = 0; }
-    const u32 ntk = direct ? 2 * A.K : cap;
-    for (u32 i = lane; i < ntk; i += 32) tk[w][i] = direct ? 0u : NONE;
-    __syncwarp();
-    cascade_fill(A, a, lm, tk[w], tc[w], td[w], cap, lane, 32);
-    __syncwarp();
-    cascade_slots(A, mvs[w], sl[w], m, tk[w], cap, lane, 32);
-    __syncwarp();
-    cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], direct ? tk[w] : nullptr);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -2765,10 +2793,11 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     run_gains(c, L, lp, A, cs);
     // counters on the device: [0] M movers, [1] 2M size events, [2] inbound transitions,
     // [3] cascade hyperedges for the block kernel, [4] for the scratch kernel, [5] for the block
-    // kernel's full-size launch after its middle tier
+    // kernel's full-size launch after its middle tier, [6] hyperedges holding a mover
     u32 *cnt = c.arena.alloc<u32>(8);
     AXC_CUDA(cudaMemsetAsync(cnt, 0, 32, c.stream));
     u32 *dM = cnt, *dSE = cnt + 1, *dT = cnt + 2, *dBig = cnt + 3, *dHuge = cnt + 4, *dBig2 = cnt + 5;
+    u32 *dHl = cnt + 6;  // hyperedges holding a mover
     // small levels: ranking, validity and the best prefix in one block each (SMALL_*)
     const bool small = rp.K <= VS_MAX_K && n <= (u32)RSS_CAP && rp.copies == 1;
     // movers in id order, then ranked by (gain desc, id asc)
@@ -2846,12 +2875,21 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         C.tdense = tdense; C.dense_stride = n;
         C.status = c.d_status;
         C.K = rp.K;
+        C.pbytes = c.profiling("k_cascade_warp") ? c.d_prof_bytes() : nullptr;
         const bool direct = rp.K <= CC_DIRECT_K;
         size_t m1 = c.arena.mark();
         u32 *big = c.arena.alloc<u32>(L.e ? L.e : 1), *huge = c.arena.alloc<u32>(L.e ? L.e : 1);
         u32 *big2 = c.arena.alloc<u32>(L.e ? L.e : 1);
         if (L.e) {
-            LAUNCH(c, k_cascade_warp, cdiv(L.e, CC_WARPS), CC_WARPS * 32, 0, C, big, dBig);
+            // only the hyperedges that hold a mover: flagged from the movers' incidences
+            u32 *hflag = c.arena.alloc<u32>(L.e), *hlist = c.arena.alloc<u32>(L.e);
+            AXC_CUDA(cudaMemsetAsync(hflag, 0, (size_t)L.e * 4, c.stream));
+            LAUNCH(c, k_mover_hedges, (u32)c.sms * 8, 256, 0, mv, dM, L.toff, L.touch, hflag);
+            compact_indices_dn(c, hflag, hlist, L.e, dHl);
+            int per_w = 1;
+            AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_w, k_cascade_warp, CC_WARPS * 32, 0));
+            const u32 gw = std::min<u32>(cdiv(L.e, CC_WARPS), (u32)c.sms * (u32)std::max(per_w, 1));
+            LAUNCH(c, k_cascade_warp, gw, CC_WARPS * 32, 0, C, hlist, dHl, big, dBig);
             // block kernel: shared memory sized by the level's largest hyperedge, all resident blocks
             u32 smov = 128;
             while (smov < lp.max_len && smov < cascade_block_movers(c)) smov <<= 1;

@@ -72,9 +72,9 @@ WORKLOADS = {
         ref=["-k", "128", "0.03", "-rfr", "16", "-cnc", "4", "-dtc", "-v", "0", "-smh", "0"],
         grade=["-k-prt", "128", "0.03"]),
 }
-DEFAULT_WORKLOAD = "snn-8x512"
+DEFAULT_WORKLOAD = "circuit-200k-k2"
 # the other configurations, measured in the same run as per-config sub-results of the line
-DEFAULT_CONFIGS = ["circuit-200k-k2", "circuit-200k-k64", "snn-1m-k128"]
+DEFAULT_CONFIGS = ["snn-8x512", "circuit-200k-k64", "snn-1m-k128", "snn-1m-incc"]
 METRIC = "pins/s end-to-end at equal lambda-1"
 L2_NOTE = "cold between timed steps: a 256 MiB write flushes L2 (the reference arm runs a fresh process per step)"
 GEN = os.path.join(ROOT, "axoncuda_b200", "axc_gen")
@@ -217,7 +217,9 @@ def barrier(world):
         dist.barrier()
 
 
-ROOFLINE_KERNEL = "k_rate_block"  # the kernel with the largest share of device time at the default workload
+# the kernel with the largest share of device time (ncu launch lists in profiles/) per workload
+ROOFLINE_KERNELS = {"circuit-200k-k2": "k_cascade_warp", "circuit-200k-k64": "k_cascade_warp",
+                    "snn-8x512": "k_rate_block", "snn-1m-k128": "k_rate_block"}
 # algorithmic bytes per launch of the kernels the library's timer has a byte model for
 BYTE_MODELS = {
     "k_rate_block": "4 B per pin visit of the listed nodes (the pin id) + 8 B per candidate slot written",
@@ -225,6 +227,10 @@ BYTE_MODELS = {
     "k_gain_block": "8 B per incidence entry of the listed nodes + 16 B per listed node",
     "k_gain_mask_warp": "8 B per incidence entry of the listed nodes + 16 B per listed node",
     "k_gain_mask_block": "8 B per incidence entry of the listed nodes + 16 B per listed node",
+    "k_cascade_warp": "per listed hyperedge (those holding a mover), counted by the kernel: 24 B (list entry, "
+                      "offsets, source count) + 8 B per pin (id, rank) + 4 B (census size), then 4 B (hand-off "
+                      "to the block kernel) or 12 B per census entry + 16 B per mover (partition, target, "
+                      "cascaded gain) + 4 B (weight); inbound transitions not counted",
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch from one ncu capture of the
 # kernel on the workload, recorded with its capture command in profiles/<kernel>-<workload>.md
@@ -389,7 +395,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     ctx = ax.Context(local, int(args.arena_gb * (1 << 30)))
     td = tempfile.mkdtemp(prefix="axc_bench_")
-    kname = args.roofline_kernel
+    kname = args.roofline_kernel or ROOFLINE_KERNELS.get(args.workload, "k_rate_block")
     head = measure_ours(ctx, args.workload, args.steps, args.warmup, world, td, roofline_kernel=kname)
     peak, peak_kind = hbm_peak()
     kt = head.pop("kernel")
@@ -699,7 +705,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--roofline-kernel", default=ROOFLINE_KERNEL)
+    ap.add_argument("--roofline-kernel", default=None,
+                    help="kernel timed for the roofline (default: the workload's largest, ROOFLINE_KERNELS)")
     ap.add_argument("--ref-timeout", type=float, default=900.0,
                     help="seconds one reference partition may take before its arm reports unavailable")
     ap.add_argument("--mode", default="partition", choices=["partition", "batch", "serve"],
