@@ -53,6 +53,8 @@ struct Error : std::runtime_error {
 
 // Bump allocator over one device allocation made when the context is created. Levels of the
 // multilevel hierarchy are strictly nested, so allocation is LIFO: `mark()` / `release()`.
+constexpr unsigned PROF_SLOTS = 16;  // device byte counters (8 B each, at byte 64 of the status allocation)
+
 struct Arena {
     char *base = nullptr;
     size_t cap = 0, top = 0, peak = 0;
@@ -108,8 +110,9 @@ struct Ctx {
     u32 prof_launches = 0;
     bool capturing = false;
     bool profiling(const char *name) const { return prof_on && prof_name == name; }
-    // Device-side byte counter of the kernels whose algorithmic bytes depend on device data (they
-    // add them while profiled): a word of the status allocation, read and cleared by profile reads.
+    // Device-side byte counters of the kernels whose algorithmic bytes depend on device data (they
+    // add them while profiled, each warp to one of PROF_SLOTS words to spread the atomics): words of
+    // the status allocation, summed and cleared by profile reads.
     unsigned long long *d_prof_bytes() const { return (unsigned long long *)((char *)d_status + 64); }
     cudaEvent_t prof_event() {
         if (prof_used == prof_ev.size()) {

@@ -333,7 +333,7 @@ int axc_profile_kernel(axc_ctx *ctx, const char *kernel) {
     c.prof_bytes = 0;
     c.prof_ms = 0;
     c.prof_launches = 0;
-    if (c.d_status && cudaMemset(c.d_prof_bytes(), 0, 8) != cudaSuccess) return AXC_ECUDA;
+    if (c.d_status && cudaMemset(c.d_prof_bytes(), 0, 8 * PROF_SLOTS) != cudaSuccess) return AXC_ECUDA;
     return AXC_OK;
 }
 
@@ -344,9 +344,10 @@ int axc_profile_read(axc_ctx *ctx, axc_kernel_timing *out) {
     try {
         AXC_CUDA(cudaStreamSynchronize(c.stream));
         c.prof_collect(0, c.prof_used);
-        unsigned long long dev_bytes = 0;  // bytes the profiled kernel counted on the device
-        AXC_CUDA(cudaMemcpy(&dev_bytes, c.d_prof_bytes(), 8, cudaMemcpyDeviceToHost));
-        AXC_CUDA(cudaMemset(c.d_prof_bytes(), 0, 8));
+        unsigned long long slots[PROF_SLOTS], dev_bytes = 0;  // bytes the profiled kernel counted
+        AXC_CUDA(cudaMemcpy(slots, c.d_prof_bytes(), sizeof slots, cudaMemcpyDeviceToHost));
+        AXC_CUDA(cudaMemset(c.d_prof_bytes(), 0, sizeof slots));
+        for (unsigned i = 0; i < PROF_SLOTS; ++i) dev_bytes += slots[i];
         out->launches = c.prof_launches;
         out->ms_total = c.prof_ms;
         out->bytes = c.prof_bytes + dev_bytes;

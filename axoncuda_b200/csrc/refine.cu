@@ -68,6 +68,8 @@ struct CensusArgs {
     // with destination pins, mw words each
     u32 *mask, *dmask;
     u32 mw;
+    // when set (kernel timer on k_census_direct_warp): each hyperedge's algorithmic bytes are added
+    unsigned long long *pbytes;
 };
 
 // insert phase: keys = partition, mn = first position, cnt/dcnt counters
@@ -190,18 +192,25 @@ __device__ __forceinline__ void cd_count(const CensusArgs &A, u64 a, u64 b, u64 
         if (k >= s) atomicAdd(&dcnt[q], 1u);
     }
 }
-__device__ __forceinline__ void cd_save(const CensusArgs &A, u32 h, u64 a, u64 b, const u32 *cnt, u32 t0, u32 nt) {
-    if (!A.save) return;
+// Returns how many savings this thread added.
+__device__ __forceinline__ u32 cd_save(const CensusArgs &A, u32 h, u64 a, u64 b, const u32 *cnt, u32 t0, u32 nt) {
+    if (!A.save) return 0;
     const u32 w = A.wfx[h];
+    u32 added = 0;
     for (u64 k = a + t0; k < b; k += nt) {
         const u32 v = A.pins[k];
         const i64 g = leave_gain(A.encourage, w, cnt[A.part[v]]);
-        if (g) atomicAdd(&A.save[v], (unsigned long long)g);
+        if (g) {
+            atomicAdd(&A.save[v], (unsigned long long)g);
+            ++added;
+        }
     }
+    return added;
 }
 // One warp: the nonzero counters in ascending partition order, then lam. The ballots of the
 // counters are the hyperedge's masks, written when A.mask is set.
-__device__ __forceinline__ void cd_emit(const CensusArgs &A, u32 h, u64 a, const u32 *cnt, const u32 *dcnt, u32 K) {
+// Returns the entries written (lam).
+__device__ __forceinline__ u32 cd_emit(const CensusArgs &A, u32 h, u64 a, const u32 *cnt, const u32 *dcnt, u32 K) {
     const u32 lane = threadIdx.x & 31;
     u32 o = 0;
     const u32 qend = A.mask ? 32 * A.mw : K;
@@ -225,22 +234,29 @@ __device__ __forceinline__ void cd_emit(const CensusArgs &A, u32 h, u64 a, const
         o += __popc(bal);
     }
     if (lane == 0) A.lam[h] = o;
+    return o;
 }
 
 __global__ void k_census_direct_warp(u32 e, CensusArgs A, u32 K) {
     __shared__ u32 tc[CS_WARPS][CD_K], td[CS_WARPS][CD_K];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u32 h = blockIdx.x * CS_WARPS + w;
-    if (h >= e) return;
-    const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
-    if (b - a > CD_WARP_LEN) return;
-    u32 *cnt = tc[w], *dcnt = td[w];
-    for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; }
-    __syncwarp();
-    cd_count(A, a, b, s, cnt, dcnt, lane, 32);
-    __syncwarp();
-    cd_save(A, h, a, b, cnt, lane, 32);
-    cd_emit(A, h, a, cnt, dcnt, K);
+    u64 bytes = 0;  // algorithmic bytes of this warp's hyperedges (kernel timer)
+    for (u32 h = blockIdx.x * CS_WARPS + w; h < e; h += gridDim.x * CS_WARPS) {
+        const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+        if (b - a > CD_WARP_LEN) continue;
+        u32 *cnt = tc[w], *dcnt = td[w];
+        __syncwarp();  // the previous hyperedge's counters are no longer read
+        for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; }
+        __syncwarp();
+        cd_count(A, a, b, s, cnt, dcnt, lane, 32);
+        __syncwarp();
+        const u32 saved = __reduce_add_sync(0xFFFFFFFFu, cd_save(A, h, a, b, cnt, lane, 32));
+        const u32 lm = cd_emit(A, h, a, cnt, dcnt, K);
+        // offsets and source count, each pin's id and partition, the entries and their count, the
+        // masks, the weight and the savings added
+        bytes += 20 + 8 * (b - a) + 12ull * lm + 4 + (A.mask ? 8ull * A.mw : 0) + (A.save ? 4 + 8ull * saved : 0);
+    }
+    if (A.pbytes && lane == 0 && bytes) atomicAdd(&A.pbytes[(blockIdx.x * CS_WARPS + w) & (PROF_SLOTS - 1)], bytes);
 }
 
 __global__ void k_census_direct_block(const u32 *__restrict__ list, u32 nlist, CensusArgs A, u32 K) {
@@ -279,6 +295,22 @@ __global__ void k_part_sizes(u32 n, const u32 *__restrict__ part, const u32 *__r
                              unsigned long long *__restrict__ ps) {
     u32 v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) atomicAdd(&ps[part[v]], (unsigned long long)nsize[v]);
+}
+// Few partitions (K <= PS_SMEM_K): per-block sums in shared memory, one global add per partition
+// and block, over a grid-stride range (every node's global atomic would hit the same K words).
+constexpr u32 PS_SMEM_K = 1024;
+__global__ void k_part_sizes_smem(u32 n, u32 K, const u32 *__restrict__ part, const u32 *__restrict__ nsize,
+                                  unsigned long long *__restrict__ ps) {
+    __shared__ unsigned long long sh[PS_SMEM_K];
+    for (u32 i = threadIdx.x; i < K; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (u32 v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const u32 q = part[v];
+        if (q < K) atomicAdd(&sh[q], (unsigned long long)nsize[v]);  // ids are below K by contract
+    }
+    __syncthreads();
+    for (u32 i = threadIdx.x; i < K; i += blockDim.x)
+        if (sh[i]) atomicAdd(&ps[i], sh[i]);
 }
 __global__ void k_part_inbound(u32 e, const u64 *__restrict__ off, const u32 *__restrict__ lam,
                                const u32 *__restrict__ cpart, const u32 *__restrict__ cdcnt,
@@ -1704,6 +1736,7 @@ __global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, cons
     __shared__ u32 tk[CC_WARPS][CC_TAB], tc[CC_WARPS][CC_TAB], td[CC_WARPS][CC_TAB];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 nl = *nlist;
+    u64 bytes = 0;  // algorithmic bytes of this warp's hyperedges (kernel timer)
     for (u32 idx = blockIdx.x * CC_WARPS + w; idx < nl; idx += gridDim.x * CC_WARPS) {
         __syncwarp();  // the previous hyperedge's shared state is no longer read
         const u32 h = list[idx];
@@ -1726,7 +1759,7 @@ __global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, cons
         // each mover's partition, target and cascaded gain, and the weight (transitions not counted)
         const u64 bytes_read = 24 + 8 * (b - a);
         if (m == 0) {  // (a listed hyperedge always has a mover)
-            if (A.pbytes && lane == 0) atomicAdd(A.pbytes, (unsigned long long)bytes_read);
+            bytes += bytes_read;
             continue;
         }
         const u32 lm = A.lam[h];
@@ -1734,11 +1767,10 @@ __global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, cons
         const u32 cap = direct ? A.K : cascade_cap32(lm, m);
         if (m > CC_MOV || cap > CC_TAB) {
             if (lane == 0) big[atomicAdd(nbig, 1u)] = h;  // handled by the block kernel
-            if (A.pbytes && lane == 0) atomicAdd(A.pbytes, (unsigned long long)(bytes_read + 8));
+            bytes += bytes_read + 8;
             continue;
         }
-        if (A.pbytes && lane == 0)
-            atomicAdd(A.pbytes, (unsigned long long)(bytes_read + 8 + 12ull * lm + 16ull * m));
+        bytes += bytes_read + 8 + 12ull * lm + 16ull * m;
         __syncwarp();
         // sort movers by rank: each key's position is the number of smaller keys (keys are unique)
         u64 mine[CC_MOV / 32];
@@ -1764,6 +1796,7 @@ __global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, cons
         __syncwarp();
         cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], direct ? tk[w] : nullptr);
     }
+    if (A.pbytes && lane == 0 && bytes) atomicAdd(&A.pbytes[(blockIdx.x * CC_WARPS + w) & (PROF_SLOTS - 1)], bytes);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -2547,12 +2580,16 @@ static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
     cs.beg = L.off;
     if (L.e == 0) return;
     CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status,
-                 (unsigned long long *)cs.save, cs.wfx, cs.encourage, nullptr, nullptr, 0};
+                 (unsigned long long *)cs.save, cs.wfx, cs.encourage, nullptr, nullptr, 0, nullptr};
+    if (c.profiling("k_census_direct_warp")) A.pbytes = c.d_prof_bytes();
     if (lp.census_K) {
         A.mask = cs.mask;  // masks come with the partition-indexed census
         A.dmask = cs.dmask;
         A.mw = cs.mw;
-        LAUNCH(c, k_census_direct_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A, lp.census_K);
+        int per_sm = 1;  // resident blocks: the warps loop over the hyperedges
+        AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_census_direct_warp, CS_WARPS * 32, 0));
+        LAUNCH(c, k_census_direct_warp, std::min<u32>(cdiv(L.e, CS_WARPS), (u32)c.sms * (u32)std::max(per_sm, 1)),
+               CS_WARPS * 32, 0, L.e, A, lp.census_K);
         if (lp.n_hblock)
             LAUNCH(c, k_census_direct_block, lp.n_hblock, 256, 0, lp.hblock, lp.n_hblock, A, lp.census_K);
         return;
@@ -2704,7 +2741,11 @@ Census build_census(Ctx &c, const DLevel &L, const u32 *part) {
 
 void part_sizes(Ctx &c, u32 n, const u32 *part, const u32 *nsize, u64 *psize, u32 K) {
     AXC_CUDA(cudaMemsetAsync(psize, 0, (size_t)K * 8, c.stream));
-    if (n) LAUNCH(c, k_part_sizes, cdiv(n, 256), 256, 0, n, part, nsize, (unsigned long long *)psize);
+    if (n && K <= PS_SMEM_K)
+        LAUNCH(c, k_part_sizes_smem, std::min<u32>(cdiv(n, 256), (u32)c.sms * 4), 256, 0, n, K, part, nsize,
+               (unsigned long long *)psize);
+    else if (n)
+        LAUNCH(c, k_part_sizes, cdiv(n, 256), 256, 0, n, part, nsize, (unsigned long long *)psize);
 }
 void part_inbound(Ctx &c, const DLevel &L, const Census &cs, u64 *pinb, u32 K) {
     AXC_CUDA(cudaMemsetAsync(pinb, 0, (size_t)K * 8, c.stream));

@@ -218,7 +218,7 @@ def barrier(world):
 
 
 # the kernel with the largest share of device time (ncu launch lists in profiles/) per workload
-ROOFLINE_KERNELS = {"circuit-200k-k2": "k_cascade_warp", "circuit-200k-k64": "k_cascade_warp",
+ROOFLINE_KERNELS = {"circuit-200k-k2": "k_census_direct_warp", "circuit-200k-k64": "k_census_direct_warp",
                     "snn-8x512": "k_rate_block", "snn-1m-k128": "k_rate_block"}
 # algorithmic bytes per launch of the kernels the library's timer has a byte model for
 BYTE_MODELS = {
@@ -231,6 +231,9 @@ BYTE_MODELS = {
                       "offsets, source count) + 8 B per pin (id, rank) + 4 B (census size), then 4 B (hand-off "
                       "to the block kernel) or 12 B per census entry + 16 B per mover (partition, target, "
                       "cascaded gain) + 4 B (weight); inbound transitions not counted",
+    "k_census_direct_warp": "per hyperedge, counted by the kernel: 20 B (offsets, source count) + 8 B per pin (id, "
+                            "partition) + 12 B per census entry written + 4 B (its count) + 8 B per mask word pair "
+                            "+ 4 B (weight) + 8 B per nonzero saving added to a pin's node",
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch from one ncu capture of the
 # kernel on the workload, recorded with its capture command in profiles/<kernel>-<workload>.md

@@ -152,8 +152,8 @@ const char *axc_last_error(axc_ctx *ctx);   /* human-readable detail of the last
  * with host clocks, sources/main.cu:151-910) ------------------------------------------------------
  * While a kernel name is set, every launch of that kernel on the context stream is bracketed by a
  * pair of CUDA events, and launch sites with a byte model add the launch's algorithmic bytes:
- * k_rate_block and the gain kernels from host-side sizes, k_cascade_warp counted by the kernel
- * itself (it depends on each round's movers). axc_profile_read synchronizes the stream, returns
+ * k_rate_block and the gain kernels from host-side sizes; k_cascade_warp and k_census_direct_warp
+ * counted by the kernels themselves (they depend on each round's movers and census). axc_profile_read synchronizes the stream, returns
  * the totals since the kernel was set and resets them. kernel = NULL switches the timer off. */
 typedef struct {
     uint32_t launches;  /* launches of the kernel seen */
