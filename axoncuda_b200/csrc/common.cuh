@@ -53,7 +53,14 @@ struct Error : std::runtime_error {
 
 // Bump allocator over one device allocation made when the context is created. Levels of the
 // multilevel hierarchy are strictly nested, so allocation is LIFO: `mark()` / `release()`.
-constexpr unsigned PROF_SLOTS = 16;  // device byte counters (8 B each, at byte 64 of the status allocation)
+// Device byte counters of the kernel timer: PROF_SLOTS words, one per 128-byte line (PROF_STRIDE
+// words apart) from byte STATUS_PROF_OFF of the status allocation, so that warps adding their
+// bytes spread over as many L2 lines.
+constexpr unsigned PROF_SLOTS = 32, PROF_STRIDE = 16, STATUS_PROF_OFF = 256;
+constexpr size_t STATUS_BYTES = STATUS_PROF_OFF + (size_t)PROF_SLOTS * PROF_STRIDE * 8;
+__device__ __forceinline__ void prof_add(unsigned long long *base, unsigned slot, unsigned long long v) {
+    atomicAdd(&base[(slot & (PROF_SLOTS - 1)) * PROF_STRIDE], v);
+}
 
 struct Arena {
     char *base = nullptr;
@@ -111,9 +118,8 @@ struct Ctx {
     bool capturing = false;
     bool profiling(const char *name) const { return prof_on && prof_name == name; }
     // Device-side byte counters of the kernels whose algorithmic bytes depend on device data (they
-    // add them while profiled, each warp to one of PROF_SLOTS words to spread the atomics): words of
-    // the status allocation, summed and cleared by profile reads.
-    unsigned long long *d_prof_bytes() const { return (unsigned long long *)((char *)d_status + 64); }
+    // add them while profiled, through prof_add): summed and cleared by profile reads.
+    unsigned long long *d_prof_bytes() const { return (unsigned long long *)((char *)d_status + STATUS_PROF_OFF); }
     cudaEvent_t prof_event() {
         if (prof_used == prof_ev.size()) {
             cudaEvent_t e;

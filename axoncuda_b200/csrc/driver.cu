@@ -305,8 +305,8 @@ int axc_create(int device, size_t arena_bytes, axc_ctx **out) {
         }
         AXC_CUDA(cudaMalloc(&c.arena.base, arena_bytes));
         c.arena.cap = arena_bytes;
-        AXC_CUDA(cudaMalloc(&c.d_status, 256));
-        AXC_CUDA(cudaMemset(c.d_status, 0, 256));
+        AXC_CUDA(cudaMalloc(&c.d_status, STATUS_BYTES));
+        AXC_CUDA(cudaMemset(c.d_status, 0, STATUS_BYTES));
         AXC_CUDA(cudaHostAlloc((void **)&c.h_pinned, 4096, cudaHostAllocDefault));
         setup_construct_kernels();
         setup_prim_kernels();
@@ -333,7 +333,8 @@ int axc_profile_kernel(axc_ctx *ctx, const char *kernel) {
     c.prof_bytes = 0;
     c.prof_ms = 0;
     c.prof_launches = 0;
-    if (c.d_status && cudaMemset(c.d_prof_bytes(), 0, 8 * PROF_SLOTS) != cudaSuccess) return AXC_ECUDA;
+    if (c.d_status && cudaMemset(c.d_prof_bytes(), 0, 8ull * PROF_SLOTS * PROF_STRIDE) != cudaSuccess)
+        return AXC_ECUDA;
     return AXC_OK;
 }
 
@@ -344,10 +345,10 @@ int axc_profile_read(axc_ctx *ctx, axc_kernel_timing *out) {
     try {
         AXC_CUDA(cudaStreamSynchronize(c.stream));
         c.prof_collect(0, c.prof_used);
-        unsigned long long slots[PROF_SLOTS], dev_bytes = 0;  // bytes the profiled kernel counted
+        unsigned long long slots[PROF_SLOTS * PROF_STRIDE], dev_bytes = 0;  // bytes the profiled kernel counted
         AXC_CUDA(cudaMemcpy(slots, c.d_prof_bytes(), sizeof slots, cudaMemcpyDeviceToHost));
         AXC_CUDA(cudaMemset(c.d_prof_bytes(), 0, sizeof slots));
-        for (unsigned i = 0; i < PROF_SLOTS; ++i) dev_bytes += slots[i];
+        for (unsigned i = 0; i < PROF_SLOTS; ++i) dev_bytes += slots[i * PROF_STRIDE];
         out->launches = c.prof_launches;
         out->ms_total = c.prof_ms;
         out->bytes = c.prof_bytes + dev_bytes;
@@ -572,8 +573,8 @@ Lane *lane_create(int device, int *rc) {
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
         c.coop_supported = coop;
         AXC_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-        AXC_CUDA(cudaMalloc(&c.d_status, 256));
-        AXC_CUDA(cudaMemset(c.d_status, 0, 256));
+        AXC_CUDA(cudaMalloc(&c.d_status, STATUS_BYTES));
+        AXC_CUDA(cudaMemset(c.d_status, 0, STATUS_BYTES));
         AXC_CUDA(cudaHostAlloc((void **)&c.h_pinned, 4096, cudaHostAllocDefault));
         scan_state_create(c, 1u << 18);
         // freed job arenas stay in the pool for the next job instead of going back to the driver

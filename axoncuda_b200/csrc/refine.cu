@@ -240,23 +240,21 @@ __device__ __forceinline__ u32 cd_emit(const CensusArgs &A, u32 h, u64 a, const 
 __global__ void k_census_direct_warp(u32 e, CensusArgs A, u32 K) {
     __shared__ u32 tc[CS_WARPS][CD_K], td[CS_WARPS][CD_K];
     const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    u64 bytes = 0;  // algorithmic bytes of this warp's hyperedges (kernel timer)
-    for (u32 h = blockIdx.x * CS_WARPS + w; h < e; h += gridDim.x * CS_WARPS) {
-        const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
-        if (b - a > CD_WARP_LEN) continue;
-        u32 *cnt = tc[w], *dcnt = td[w];
-        __syncwarp();  // the previous hyperedge's counters are no longer read
-        for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; }
-        __syncwarp();
-        cd_count(A, a, b, s, cnt, dcnt, lane, 32);
-        __syncwarp();
-        const u32 saved = __reduce_add_sync(0xFFFFFFFFu, cd_save(A, h, a, b, cnt, lane, 32));
-        const u32 lm = cd_emit(A, h, a, cnt, dcnt, K);
-        // offsets and source count, each pin's id and partition, the entries and their count, the
-        // masks, the weight and the savings added
-        bytes += 20 + 8 * (b - a) + 12ull * lm + 4 + (A.mask ? 8ull * A.mw : 0) + (A.save ? 4 + 8ull * saved : 0);
-    }
-    if (A.pbytes && lane == 0 && bytes) atomicAdd(&A.pbytes[(blockIdx.x * CS_WARPS + w) & (PROF_SLOTS - 1)], bytes);
+    const u32 h = blockIdx.x * CS_WARPS + w;
+    if (h >= e) return;
+    const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+    if (b - a > CD_WARP_LEN) return;
+    u32 *cnt = tc[w], *dcnt = td[w];
+    for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; }
+    __syncwarp();
+    cd_count(A, a, b, s, cnt, dcnt, lane, 32);
+    __syncwarp();
+    const u32 saved = __reduce_add_sync(0xFFFFFFFFu, cd_save(A, h, a, b, cnt, lane, 32));
+    const u32 lm = cd_emit(A, h, a, cnt, dcnt, K);
+    if (A.pbytes && lane == 0)  // algorithmic bytes (kernel timer): offsets and source count, each
+        // pin's id and partition, the entries and their count, the masks, the weight and savings
+        prof_add(A.pbytes, h, 20 + 8 * (b - a) + 12ull * lm + 4 + (A.mask ? 8ull * A.mw : 0) +
+                                  (A.save ? 4 + 8ull * saved : 0));
 }
 
 __global__ void k_census_direct_block(const u32 *__restrict__ list, u32 nlist, CensusArgs A, u32 K) {
@@ -1796,7 +1794,7 @@ __global__ void k_cascade_warp(CascadeArgs A, const u32 *__restrict__ list, cons
         __syncwarp();
         cascade_sweep_warp(A, h, mvs[w], sl[w], m, tk[w], tc[w], td[w], direct ? tk[w] : nullptr);
     }
-    if (A.pbytes && lane == 0 && bytes) atomicAdd(&A.pbytes[(blockIdx.x * CC_WARPS + w) & (PROF_SLOTS - 1)], bytes);
+    if (A.pbytes && lane == 0 && bytes) prof_add(A.pbytes, blockIdx.x * CC_WARPS + w, bytes);
 }
 
 // Block-wide bitonic sort of buf[0, P) ascending (P a power of two).
@@ -2586,10 +2584,7 @@ static void run_census(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         A.mask = cs.mask;  // masks come with the partition-indexed census
         A.dmask = cs.dmask;
         A.mw = cs.mw;
-        int per_sm = 1;  // resident blocks: the warps loop over the hyperedges
-        AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_census_direct_warp, CS_WARPS * 32, 0));
-        LAUNCH(c, k_census_direct_warp, std::min<u32>(cdiv(L.e, CS_WARPS), (u32)c.sms * (u32)std::max(per_sm, 1)),
-               CS_WARPS * 32, 0, L.e, A, lp.census_K);
+        LAUNCH(c, k_census_direct_warp, cdiv(L.e, CS_WARPS), CS_WARPS * 32, 0, L.e, A, lp.census_K);
         if (lp.n_hblock)
             LAUNCH(c, k_census_direct_block, lp.n_hblock, 256, 0, lp.hblock, lp.n_hblock, A, lp.census_K);
         return;
