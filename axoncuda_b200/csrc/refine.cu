@@ -272,6 +272,121 @@ __global__ void k_census_direct_block(const u32 *__restrict__ list, u32 nlist, C
     }
 }
 
+// ---- incremental partition-indexed census (levels that are not small, K <= CD_K) ---------------
+// The level keeps one census across its rounds. Round r recomputes only the hyperedges holding a
+// node that moved in round r - 1 (all of them in round 0): their entries, count and masks are
+// rewritten, and each pin's saving changes by leave_gain(w, its partition's new count) minus
+// leave_gain(w, its partition's count at the previous census). A node's partition at the
+// previous census is its current one, unless it moved in round r - 1: then the apply kernel kept
+// the old one in prev[] and stamped the move with the round counter. The results are those of a
+// census rebuilt from scratch (integer sums, the same entries in the same order).
+struct IncArgs {
+    const u32 *list, *nlist;   // the hyperedges to recompute
+    u32 *work;                 // the warps' work counter (zeroed before the launch)
+    const u32 *dirty;          // their flags (the block kernel's filter)
+    const u32 *prev, *stamp;   // [n]
+    const u32 *ctr;            // rounds run at this level (0 in round 0)
+};
+
+// Old counts from the hyperedge's previous entries [a, a + lm) into ocnt (zeroed, K slots).
+__device__ __forceinline__ void ci_old_counts(const CensusArgs &A, u64 a, u32 lm, u32 *ocnt, u32 t0, u32 nt) {
+    for (u32 j = t0; j < lm; j += nt) ocnt[A.cpart[a + j]] = A.ccnt[a + j];
+}
+// The savings' change of pins t0, t0 + nt, ... (all of their saving in round 0); returns how many
+// this thread added.
+__device__ __forceinline__ u32 ci_save(const CensusArgs &A, const IncArgs &I, u32 h, u64 a, u64 b, const u32 *cnt,
+                                       const u32 *ocnt, u32 r, u32 t0, u32 nt) {
+    const u32 w = A.wfx[h];
+    u32 added = 0;
+    for (u64 k = a + t0; k < b; k += nt) {
+        const u32 v = A.pins[k], p = A.part[v];
+        i64 g = leave_gain(A.encourage, w, cnt[p]);
+        if (r) {
+            const u32 po = I.stamp[v] == r - 1 ? I.prev[v] : p;
+            g -= leave_gain(A.encourage, w, ocnt[po]);
+        }
+        if (g) {
+            atomicAdd(&A.save[v], (unsigned long long)g);
+            ++added;
+        }
+    }
+    return added;
+}
+
+// Listed hyperedges of at most CD_WARP_LEN pins, one warp each; warps take 32 list entries at a
+// time from a shared counter.
+__global__ void k_census_inc_warp(CensusArgs A, u32 K, IncArgs I) {
+    __shared__ u32 tc[CS_WARPS][CD_K], td[CS_WARPS][CD_K], to[CS_WARPS][CD_K];
+    const u32 w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 nl = *I.nlist, r = *I.ctr;
+    u32 *cnt = tc[w], *dcnt = td[w], *ocnt = to[w];
+    u64 bytes = 0;  // algorithmic bytes of this warp's hyperedges (kernel timer)
+    for (;;) {
+        u32 base = 0;
+        if (lane == 0) base = atomicAdd(I.work, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= nl) break;
+        const u32 end = base + 32 < nl ? base + 32 : nl;
+        for (u32 idx = base; idx < end; ++idx) {
+            const u32 h = I.list[idx];
+            const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+            if (b - a > CD_WARP_LEN) continue;  // the block kernel's
+            const u32 lm_old = r ? A.lam[h] : 0;
+            __syncwarp();  // the previous hyperedge's tables are no longer read
+            for (u32 i = lane; i < K; i += 32) { cnt[i] = 0; dcnt[i] = 0; ocnt[i] = 0; }
+            __syncwarp();
+            if (r) ci_old_counts(A, a, lm_old, ocnt, lane, 32);
+            cd_count(A, a, b, s, cnt, dcnt, lane, 32);
+            __syncwarp();  // old entries read, counts complete, before the entries are rewritten
+            const u32 saved = __reduce_add_sync(0xFFFFFFFFu, ci_save(A, I, h, a, b, cnt, ocnt, r, lane, 32));
+            const u32 lm = cd_emit(A, h, a, cnt, dcnt, K);
+            // the list entry, offsets and source count, each pin's id, partition (and move stamp),
+            // the old entries, the new entries and their count, the masks, the weight and savings
+            bytes += 24 + 12 * (b - a) + 8ull * lm_old + 12ull * lm + 4 + (A.mask ? 8ull * A.mw : 0) + 4 +
+                     8ull * saved;
+        }
+    }
+    if (A.pbytes && lane == 0 && bytes) prof_add(A.pbytes, blockIdx.x * CS_WARPS + w, bytes);
+}
+
+// Hyperedges of more than CD_WARP_LEN pins (the level's block list), one block each, when flagged.
+__global__ void k_census_inc_block(const u32 *__restrict__ list, u32 nlist, CensusArgs A, u32 K, IncArgs I) {
+    __shared__ u32 cnt[CD_K], dcnt[CD_K], ocnt[CD_K];
+    const u32 r = *I.ctr;
+    for (u32 idx = blockIdx.x; idx < nlist; idx += gridDim.x) {
+        const u32 h = list[idx];
+        if (!I.dirty[h]) continue;  // uniform over the block
+        const u64 a = A.off[h], b = A.off[h + 1], s = a + A.nsrc[h];
+        const u32 lm_old = r ? A.lam[h] : 0;
+        for (u32 i = threadIdx.x; i < K; i += blockDim.x) { cnt[i] = 0; dcnt[i] = 0; ocnt[i] = 0; }
+        __syncthreads();
+        if (r) ci_old_counts(A, a, lm_old, ocnt, threadIdx.x, blockDim.x);
+        cd_count(A, a, b, s, cnt, dcnt, threadIdx.x, blockDim.x);
+        __syncthreads();
+        ci_save(A, I, h, a, b, cnt, ocnt, r, threadIdx.x, blockDim.x);
+        __syncthreads();  // every thread has read lam and the old entries
+        if (threadIdx.x < 32) cd_emit(A, h, a, cnt, dcnt, K);
+        __syncthreads();
+    }
+}
+
+// After the apply: the hyperedges of the nodes this round moved (stamped with the round counter)
+// are flagged for the next round's census. One warp per mover.
+__global__ void k_mark_moved(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ stamp,
+                             const u32 *__restrict__ ctr, const u64 *__restrict__ toff, const u32 *__restrict__ touch,
+                             u32 *__restrict__ dirty) {
+    const u32 lane = threadIdx.x & 31u, nw = (gridDim.x * blockDim.x) >> 5;
+    const u32 M = *dM, r = *ctr;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < M; i += nw) {
+        const u32 v = mv[i];
+        if (stamp[v] != r) continue;  // not applied this round
+        for (u64 j = toff[v] + lane; j < toff[v + 1]; j += 32) dirty[touch[j]] = 1u;
+    }
+}
+__global__ void k_round_tick(u32 *ctr) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) ctr[0] += 1;
+}
+
 __global__ void k_flag_len(u32 e, const u64 *__restrict__ off, u64 lo, u64 hi, u32 *__restrict__ flag) {
     u32 h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h < e) {
@@ -2361,11 +2476,17 @@ __global__ void k_best_final(const Best *__restrict__ in, u32 nb, const i64 *__r
     const i64 vi = (has_vi && x.r != 0xFFFFFFFFu) ? seg_prefix(pre, n, 2, x.r) : 0;
     *apply = (x.r != 0xFFFFFFFFu && x.vs <= 0 && vi <= 0 && x.g >= 0) ? 1u : 0u;
 }
+// With prev set (incremental census), a moved node's old partition and the round counter are kept.
 __global__ void k_apply(const u32 *__restrict__ mv, const u32 *__restrict__ target, const Best *__restrict__ best,
-                        const u32 *__restrict__ apply, u32 *__restrict__ part) {
+                        const u32 *__restrict__ apply, u32 *__restrict__ part, u32 *__restrict__ prev,
+                        u32 *__restrict__ stamp, const u32 *__restrict__ ctr) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (!*apply || i > best->r) return;
     u32 v = mv[i];
+    if (prev) {
+        prev[v] = part[v];
+        stamp[v] = *ctr;
+    }
     part[v] = target[v];
 }
 
@@ -2407,12 +2528,17 @@ __global__ void k_best_seg(const i64 *__restrict__ pre, u32 n, int has_vi, const
 }
 __global__ void k_apply_seg(const u32 *__restrict__ mv, const u32 *__restrict__ dM, const u32 *__restrict__ ck,
                             const u32 *__restrict__ target, const Best *__restrict__ best,
-                            const u32 *__restrict__ capply, u32 *__restrict__ part) {
+                            const u32 *__restrict__ capply, u32 *__restrict__ part, u32 *__restrict__ prev,
+                            u32 *__restrict__ stamp, const u32 *__restrict__ ctr) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *dM) return;
     const u32 t = ck[i];
     if (!capply[t] || i > best[t].r) return;
     const u32 v = mv[i];
+    if (prev) {
+        prev[v] = part[v];
+        stamp[v] = *ctr;
+    }
     part[v] = target[v];
 }
 
@@ -2465,6 +2591,13 @@ static u32 cascade_block_movers(const Ctx &c) {
     u32 lim = 128;
     while ((unsigned long)lim * 2 <= v && lim < CB_MOV_MAX) lim <<= 1;
     return lim;
+}
+
+// The incremental census is on unless the environment variable AXC_INC_CENSUS is "0" (then every
+// round rebuilds the census; the same results).
+static bool inc_census_enabled() {
+    const char *s = std::getenv("AXC_INC_CENSUS");
+    return !(s && s[0] == '0');
 }
 
 static bool round_loop_enabled() {
@@ -2805,16 +2938,75 @@ void refine_gains_only(Ctx &c, const DLevel &L, const u32 *wfx, const RefinePara
     c.arena.release(m);
 }
 
+// The level-persistent census of the incremental rounds (k_census_inc_*), for levels with a
+// partition-indexed census (K <= CD_K) that are not small.
+struct IncCensus {
+    Census cs;              // entries, counts, masks and node savings, kept across the rounds
+    u32 *dirty = nullptr;   // [e] hyperedges to recompute at the next census (all before round 0)
+    u32 *dlist = nullptr;   // [e] their compacted list
+    u32 *prev = nullptr;    // [n] a moved node's partition before its last move
+    u32 *stamp = nullptr;   // [n] the round counter at the node's last move (NONE: none)
+    u32 *ctr = nullptr;     // [0] rounds run at this level, [1] the list count, [2] the warps' work
+};
+
+static bool inc_census_eligible(const DLevel &L, const LevelPrep &lp, const RefineParams &rp) {
+    const bool small = rp.K <= VS_MAX_K && L.n <= (u32)RSS_CAP && rp.copies == 1;
+    return lp.census_K && rp.K <= GN_DIRECT_K && !small && L.e;
+}
+
+static void inc_census_init(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp, IncCensus &ic) {
+    ic.cs = alloc_census(c, L);
+    ic.cs.save = c.arena.alloc<i64>(L.n ? L.n : 1);
+    AXC_CUDA(cudaMemsetAsync(ic.cs.save, 0, (size_t)L.n * 8, c.stream));
+    ic.cs.wfx = wfx;
+    ic.cs.encourage = rp.encourage ? 1 : 0;
+    ic.cs.mw = mask_words(rp.K);
+    ic.cs.mask = c.arena.alloc<u32>((u64)L.e * ic.cs.mw);
+    ic.cs.dmask = c.arena.alloc<u32>((u64)L.e * ic.cs.mw);
+    ic.dirty = c.arena.alloc<u32>(L.e);
+    ic.dlist = c.arena.alloc<u32>(L.e);
+    ic.prev = c.arena.alloc<u32>(L.n ? L.n : 1);
+    ic.stamp = c.arena.alloc<u32>(L.n ? L.n : 1);
+    ic.ctr = c.arena.alloc<u32>(4);
+    fill_u32(c, ic.dirty, 1u, L.e);
+    fill_u32(c, ic.stamp, NONE, L.n);
+    AXC_CUDA(cudaMemsetAsync(ic.ctr, 0, 16, c.stream));
+}
+
+// The round's census in incremental form: the flagged hyperedges are listed, recomputed and
+// unflagged.
+static void inc_census_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *part, IncCensus &ic) {
+    const Census &cs = ic.cs;
+    CensusArgs A{L.off, L.pins, L.nsrc, part, cs.part, cs.cnt, cs.dcnt, cs.lam, c.d_status,
+                 (unsigned long long *)cs.save, cs.wfx, cs.encourage, cs.mask, cs.dmask, cs.mw, nullptr};
+    if (c.profiling("k_census_inc_warp")) A.pbytes = c.d_prof_bytes();
+    compact_indices_dn(c, ic.dirty, ic.dlist, L.e, ic.ctr + 1);
+    AXC_CUDA(cudaMemsetAsync(ic.ctr + 2, 0, 4, c.stream));
+    const IncArgs I{ic.dlist, ic.ctr + 1, ic.ctr + 2, ic.dirty, ic.prev, ic.stamp, ic.ctr};
+    int per_sm = 1;
+    AXC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_census_inc_warp, CS_WARPS * 32, 0));
+    LAUNCH(c, k_census_inc_warp, std::min<u32>(cdiv(L.e, CS_WARPS), (u32)c.sms * (u32)std::max(per_sm, 1)),
+           CS_WARPS * 32, 0, A, lp.census_K, I);
+    if (lp.n_hblock) LAUNCH(c, k_census_inc_block, lp.n_hblock, 256, 0, lp.hblock, lp.n_hblock, A, lp.census_K, I);
+    AXC_CUDA(cudaMemsetAsync(ic.dirty, 0, (size_t)L.e * 4, c.stream));
+}
+
 // The launches of one round, with no host synchronization: safe to capture in a CUDA graph.
 // dyn (device, optional) holds the round's discount and round number for graph replays. Returns
 // the device word that says whether the moves were applied; its arena slot lies below `keep`,
 // the mark the caller releases to after reading it.
 static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
-                       u32 *part, u32 discount, u32 round, const u32 *dyn, size_t &keep) {
+                       u32 *part, u32 discount, u32 round, const u32 *dyn, size_t &keep, IncCensus *ic) {
     const u32 n = L.n;
     u32 *apply = c.arena.alloc<u32>(1);
     keep = c.arena.mark();
-    Census cs = census_for_gains(c, L, lp, wfx, rp, part);
+    Census cs;
+    if (ic) {
+        inc_census_round(c, L, lp, part, *ic);
+        cs = ic->cs;
+    } else {
+        cs = census_for_gains(c, L, lp, wfx, rp, part);
+    }
     u64 *psize = c.arena.alloc<u64>(rp.K), *pinb = c.arena.alloc<u64>(rp.K);
     part_sizes(c, n, part, L.nsize, psize, rp.K);
     if (inbound_binds(L, rp)) {
@@ -3026,13 +3218,19 @@ static u32 *round_body(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *
         u32 *capply = c.arena.alloc<u32>(rp.copies);
         AXC_CUDA(cudaMemsetAsync(apply, 0, 4, c.stream));
         LAUNCH(c, k_best_seg, rp.copies, 256, 0, pre, n, track ? 1 : 0, dM, ck, bs, capply, apply);
-        LAUNCH(c, k_apply_seg, cdiv(n, 256), 256, 0, mv, dM, ck, target, bs, capply, part);
+        LAUNCH(c, k_apply_seg, cdiv(n, 256), 256, 0, mv, dM, ck, target, bs, capply, part, ic ? ic->prev : nullptr,
+               ic ? ic->stamp : nullptr, ic ? (const u32 *)ic->ctr : nullptr);
     } else {
         const u32 nbk = cdiv(n, 256) < 64u ? cdiv(n, 256) : 64u;
         Best *bb = (Best *)c.arena.alloc<u64>(4 * (nbk + 1));
         LAUNCH(c, k_best, nbk, 256, 0, pre, n, track ? 1 : 0, dM, bb + 1);
         LAUNCH(c, k_best_final, 1, 1, 0, bb + 1, nbk, pre, n, track ? 1 : 0, bb, apply);
-        LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part);
+        LAUNCH(c, k_apply, cdiv(n, 256), 256, 0, mv, target, bb, apply, part, ic ? ic->prev : nullptr,
+               ic ? ic->stamp : nullptr, ic ? (const u32 *)ic->ctr : nullptr);
+    }
+    if (ic) {  // flag the moved nodes' hyperedges for the next census, then count the round
+        LAUNCH(c, k_mark_moved, (u32)c.sms * 8, 256, 0, mv, dM, ic->stamp, ic->ctr, L.toff, L.touch, ic->dirty);
+        LAUNCH(c, k_round_tick, 1, 32, 0, ic->ctr);
     }
     c.arena.release(keep);
     return apply;
@@ -3054,10 +3252,10 @@ static bool round_result(Ctx &c, const u32 *apply) {
 
 // One round, launched eagerly; returns true when moves were applied.
 static bool refine_round(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
-                         u32 *part, u32 discount, u32 round) {
+                         u32 *part, u32 discount, u32 round, IncCensus *ic) {
     const size_t m0 = c.arena.mark();
     size_t keep;
-    const u32 *apply = round_body(c, L, lp, wfx, rp, part, discount, round, nullptr, keep);
+    const u32 *apply = round_body(c, L, lp, wfx, rp, part, discount, round, nullptr, keep, ic);
     const bool r = round_result(c, apply);
     c.arena.release(m0);
     return r;
@@ -3133,7 +3331,7 @@ __global__ void k_level_bounds(u32 e, const u64 *__restrict__ off, const u32 *__
 // (round_body) followed by k_round_next, which applies the round schedule on the device. Returns
 // the rounds run.
 static u32 refine_level_loop(Ctx &c, const DLevel &L, const LevelPrep &lp, const u32 *wfx, const RefineParams &rp,
-                             u32 *part) {
+                             u32 *part, IncCensus *ic) {
     const u32 R = rp.rounds;
     u32 *dyn = c.arena.alloc<u32>(2), *rs = c.arena.alloc<u32>(4);
     {
@@ -3166,7 +3364,7 @@ static u32 refine_level_loop(Ctx &c, const DLevel &L, const LevelPrep &lp, const
     AXC_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     c.capturing = true;
     try {
-        apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep);
+        apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep, ic);
         LAUNCH(c, k_round_next, 1, 1, 0, h, rs, dyn, apply, c.d_status);
     } catch (...) {
         c.capturing = false;
@@ -3200,6 +3398,12 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
     if (R == 0 || L.n == 0) return 0;
     size_t m = c.arena.mark();
     LevelPrep lp = prepare_level(c, L, wfx, rp.K);
+    // one census kept across the rounds where the level allows it (k_census_inc_*)
+    IncCensus icv, *ic = nullptr;
+    if (inc_census_eligible(L, lp, rp) && inc_census_enabled()) {
+        inc_census_init(c, L, wfx, rp, icv);
+        ic = &icv;
+    }
     // Graph replays need the round's scalars in device memory. Kernel-timer pairs captured in the
     // graph are read back after every replay; the bytes of the captured launches count per replay.
     const bool graph = R > 1;
@@ -3209,7 +3413,7 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
     // variable AXC_ROUND_LOOP=0 also selects the replays (the same kernels and results; profilers
     // that do not follow kernels into conditional graph nodes see them then).
     if (graph && !c.prof_on && round_loop_enabled()) {
-        const u32 done = refine_level_loop(c, L, lp, wfx, rp, part);
+        const u32 done = refine_level_loop(c, L, lp, wfx, rp, part, ic);
         c.arena.release(m);
         return done;
     }
@@ -3227,7 +3431,7 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
         AXC_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
         c.capturing = true;
         try {
-            apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep);
+            apply = round_body(c, L, lp, wfx, rp, part, 1, 0, dyn, keep, ic);
         } catch (...) {
             c.capturing = false;
             cudaGraph_t junk = nullptr;
@@ -3262,7 +3466,7 @@ u32 refine_level(Ctx &c, const DLevel &L, const u32 *wfx, const RefineParams &rp
             c.prof_collect(ev0, ev1);
             c.prof_bytes += bytes_per_round;
         } else {
-            applied = refine_round(c, L, lp, wfx, rp, part, discount, r);
+            applied = refine_round(c, L, lp, wfx, rp, part, discount, r, ic);
         }
         if (!applied) {
             if (r < R / 3) r = R / 2;

@@ -218,7 +218,7 @@ def barrier(world):
 
 
 # the kernel with the largest share of device time (ncu launch lists in profiles/) per workload
-ROOFLINE_KERNELS = {"circuit-200k-k2": "k_census_direct_warp", "circuit-200k-k64": "k_census_direct_warp",
+ROOFLINE_KERNELS = {"circuit-200k-k2": "k_census_inc_warp", "circuit-200k-k64": "k_census_inc_warp",
                     "snn-8x512": "k_rate_block", "snn-1m-k128": "k_rate_block"}
 # algorithmic bytes per launch of the kernels the library's timer has a byte model for
 BYTE_MODELS = {
@@ -234,6 +234,10 @@ BYTE_MODELS = {
     "k_census_direct_warp": "per hyperedge, counted by the kernel: 20 B (offsets, source count) + 8 B per pin (id, "
                             "partition) + 12 B per census entry written + 4 B (its count) + 8 B per mask word pair "
                             "+ 4 B (weight) + 8 B per nonzero saving added to a pin's node",
+    "k_census_inc_warp": "per recomputed hyperedge, counted by the kernel: 24 B (list entry, offsets, source count) "
+                         "+ 12 B per pin (id, partition, move stamp) + 8 B per old census entry read + 12 B per "
+                         "entry written + 4 B (its count) + 8 B per mask word pair + 4 B (weight) + 8 B per "
+                         "nonzero saving change",
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch from one ncu capture of the
 # kernel on the workload, recorded with its capture command in profiles/<kernel>-<workload>.md

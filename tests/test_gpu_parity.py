@@ -189,6 +189,21 @@ def test_refine_rounds_match_oracle(ctx, name, encourage, K, omega, delta, round
     assert 1 <= ran <= rounds and (out != part).any()
 
 
+# The same on a level above the small-level bound (20,000 nodes, K <= 256): the rounds keep one
+# census and recompute only the hyperedges of the previous round's moved nodes.
+@pytest.mark.parametrize("rounds", [1, 2, 3, 6])
+@pytest.mark.parametrize("encourage,K,omega,delta", [(False, 8, 4000, 1 << 20), (True, 200, 300, 1500)])
+def test_refine_rounds_large_level_match_oracle(ctx, encourage, K, omega, delta, rounds):
+    g = dedup(ax.gen_circuit(20000, 22000, 2, 64, 2.5, 0.9, 0.02, 5))
+    rng = np.random.default_rng(rounds + 10)
+    part = rng.integers(0, K, g.n).astype(np.uint32)
+    ns = rng.integers(1, 3, g.n).astype(np.uint32)
+    out, ran = ctx.stage_refine(g, part, K, ns, omega, delta, encourage, rounds, 3)
+    o = O.refine(g.n, g.off, g.pins, g.nsrc, O.wfx(g.w), ns, part, K, omega, delta, encourage, rounds, 3)
+    np.testing.assert_array_equal(out, o)
+    assert 1 <= ran <= rounds and (out != part).sum() > 1000
+
+
 def test_refine_two_rounds_discount_matches_oracle(ctx):
     """Two rounds from a refined partition in which every node has a move: round 0 runs at
     discount 2, and the oracle applies one move in each round."""
