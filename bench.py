@@ -241,7 +241,8 @@ BYTE_MODELS = {
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch from one ncu capture of the
 # kernel on the workload, recorded with its capture command in profiles/<kernel>-<workload>.md
-PROFILED_TRAFFIC = {("k_rate_block", "snn-8x512"): 616456, ("k_census_direct_warp", "circuit-200k-k2"): 67656819}
+PROFILED_TRAFFIC = {("k_rate_block", "snn-8x512"): 616456, ("k_census_direct_warp", "circuit-200k-k2"): 67656819,
+                    ("k_census_inc_warp", "circuit-200k-k2"): 22632375}
 STEP_MODEL = ("construction 8P+8(n+E); per rated level 4 B per rating pin visit + 4P_l + 16 n_l C (matching); "
               "per contraction 8P_l + 12P_(l+1); per refinement round 16P_l + 16n_l (moves not counted)")
 
