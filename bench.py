@@ -247,6 +247,15 @@ STEP_MODEL = ("construction 8P+8(n+E); per rated level 4 B per rating pin visit 
               "per contraction 8P_l + 12P_(l+1); per refinement round 16P_l + 16n_l (moves not counted)")
 
 
+def sub_configs(arg: str | None, world: int) -> list[str]:
+    """The other configurations measured as sub-results: the given comma-separated list ('none'
+    for none), or by default DEFAULT_CONFIGS on one GPU and none under torchrun, where the
+    scaling runs time the line's workload alone."""
+    if arg is None:
+        return list(DEFAULT_CONFIGS) if world == 1 else []
+    return [] if arg == "none" else [x for x in arg.split(",") if x]
+
+
 def hbm_peak() -> tuple[float, str]:
     """Measured copy bandwidth of this pool's B200s (GB/s), else the stated fallback."""
     try:
@@ -430,7 +439,7 @@ def run_ours(args, world, rank, local):
         out["cpu_baseline"] = grader_baseline(path, pf, args.workload, P)
     # the other configurations, fewer steps each (the step count is in each entry)
     subs = {}
-    for name in ([] if args.configs == "none" else args.configs.split(",")):
+    for name in sub_configs(args.configs, world):
         if name == args.workload:
             continue
         large = name.startswith("snn-1m")
@@ -533,7 +542,7 @@ def run_reference(args):
                  "quality": {"grader": head["graded"], "stdout_connectivity": head["stdout_connectivity"]},
                  "clocks": clk.summary()})
     subs = {}
-    for name in ([] if args.configs == "none" else args.configs.split(",")):
+    for name in sub_configs(args.configs, int(os.environ.get("WORLD_SIZE", "1"))):
         if name == args.workload:
             continue
         large = name.startswith("snn-1m")
@@ -731,8 +740,9 @@ def main():
     ap.add_argument("--seq-arena-gb", type=float, default=24.0)
     ap.add_argument("--arena-gb", type=float, default=0.0,
                     help="device arena of the partition context in GiB (0: the library default, 60%% of free memory)")
-    ap.add_argument("--configs", default=",".join(DEFAULT_CONFIGS),
-                    help="comma-separated other workloads measured as sub-results of the line, or 'none'")
+    ap.add_argument("--configs", default=None,
+                    help="comma-separated other workloads measured as sub-results of the line, or 'none' "
+                         f"(default: {','.join(DEFAULT_CONFIGS)} on one GPU, none under torchrun)")
     args = ap.parse_args()
     if args.mode == "batch":
         out = run_batch(args)

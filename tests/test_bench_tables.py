@@ -34,3 +34,10 @@ def test_default_workloads_exist_in_both_tables():
         assert name in bench.WORKLOADS, name
         assert f'"{name}"' in src, name
     assert bench.DEFAULT_WORKLOAD not in bench.DEFAULT_CONFIGS
+
+
+def test_sub_configs_default_to_one_gpu_runs():
+    assert bench.sub_configs(None, 1) == bench.DEFAULT_CONFIGS
+    assert bench.sub_configs(None, 8) == []
+    assert bench.sub_configs("none", 1) == []
+    assert bench.sub_configs("snn-8x512,circuit-200k-k64", 4) == ["snn-8x512", "circuit-200k-k64"]
